@@ -1,0 +1,411 @@
+"""Benchmark of the split-solver step on B200: cell-updates/s and % of the HBM
+roofline.
+
+Workload (one bench step): the 2-D four-quadrant Riemann problem on a
+4096 x 4096 grid over [0,1]^2, gamma = 1.4, quadrant states (rho, u, v, p)
+drawn from the seed (rho log-uniform in [0.1, 10], velocities uniform in
+[-2, 2], p log-uniform in [0.01, 1000]); dimensionally split MUSCL-Hancock
+with the van Leer limiter and pressure flattening, HLLC flux, FP64,
+transmissive boundaries, 100 time steps at CFL 0.8, the CFL reduction fused
+into the last sweep of each step.  Synthetic data (seeded), inputs resident
+in HBM when timing starts; each 537 MB state buffer exceeds the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank solves its own replica of the workload (the path
+runs independent problems; no collective on the data path) and the line
+reports the aggregate over ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GAMMA = 1.4
+SEED = 0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--size", type=int, default=4096)
+    p.add_argument("--time-steps", type=int, default=100)
+    p.add_argument("--dtype", choices=["f64", "f32"], default="f64")
+    p.add_argument("--flux", choices=["hllc", "force"], default="hllc")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-variants", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a):
+    return {
+        "workload": f"2-D four-quadrant Riemann problem {a.size}x{a.size} on [0,1]^2, "
+                    f"{a.time_steps} steps, MUSCL-Hancock + van Leer + flattening, "
+                    f"{a.flux.upper()} flux, CFL 0.8, transmissive",
+        "grid": [a.size, a.size],
+        "time_steps_per_run": a.time_steps,
+        "flux": a.flux,
+        "limiter": "vanleer",
+        "reconstruction": "muscl-hancock",
+        "seed": SEED,
+        "l2": "no flush: every state buffer (%d MB) exceeds the 126 MB L2"
+              % (a.size * a.size * 4 * (8 if a.dtype == "f64" else 4) // 2 ** 20),
+        "parallelism": "replicas" if a.gpus > 1 else "single",
+    }
+
+
+# ---- distributed plumbing ---------------------------------------------------
+
+def dist_init(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if a.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- clocks ---------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "power_w_max": max(power), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---- CPU baseline (reference functors) -------------------------------------
+
+def cpu_reference_rate(a, budget_s=12.0, max_steps=50):
+    """Times the reference's own numerics functors on the host cores on a
+    bounded sample of the workload: whole time steps of the same grid, starting
+    from the same initial state.  Returns (cell-updates/s, kind, cores, sample)."""
+    from oracle import oracle
+    from fluidity_b200.workloads import riemann_states
+    shape = (a.size, a.size)
+    u = oracle.fill_riemann(shape, riemann_states(SEED, 2), GAMMA)
+    cells = a.size * a.size
+    cores = os.cpu_count() or 1
+    if oracle.ref_available():
+        kind = "reference"
+        run = lambda n: oracle.ref_simulate(shape, u, GAMMA, 0.8, 1.0 / a.size, 1e30, n,
+                                            flux=a.flux)
+    else:
+        kind = "port"
+        cores = 1
+        run = lambda n: oracle.simulate(shape, u, GAMMA, 0.8, 1.0 / a.size, 1e30, n,
+                                        flux=a.flux)
+    t0 = time.perf_counter()
+    run(1)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(max_steps, budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    run(n)
+    dt = time.perf_counter() - t0
+    sample = (f"{n} time step(s) of the {a.size}x{a.size} FP64 {a.flux.upper()} run from its "
+              f"initial state, {cores} thread(s), {dt:.1f} s")
+    return cells * n / dt, kind, cores, sample
+
+
+def run_reference_arm(a, world, rank):
+    if rank != 0:
+        return
+    if a.dtype != "f64":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference's MUSCL reconstructor does not compile for float"}))
+        return
+    from oracle import oracle
+    from fluidity_b200.workloads import riemann_states
+    shape = (a.size, a.size)
+    cells = a.size * a.size
+    u = oracle.fill_riemann(shape, riemann_states(SEED, 2), GAMMA)
+    if oracle.ref_available():
+        kind, cores = "reference", os.cpu_count() or 1
+        step = lambda: oracle.ref_simulate(shape, u, GAMMA, 0.8, 1.0 / a.size, 1e30, 1,
+                                           flux=a.flux)
+    else:
+        kind, cores = "port", 1
+        step = lambda: oracle.simulate(shape, u, GAMMA, 0.8, 1.0 / a.size, 1e30, 1, flux=a.flux)
+    for _ in range(a.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = cells * a.steps / dt
+    sample = (f"each step: one time step (both sweeps + CFL) of the {a.size}x{a.size} FP64 "
+              f"{a.flux.upper()} run, {cores} thread(s)")
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": value,
+        "unit": "cell-updates/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
+        "config": workload_config(a),
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---- our arm ------------------------------------------------------------------
+
+def run_ours(a, world, rank, local):
+    import torch
+    from fluidity_b200 import build as fb
+    fb.build()
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    shape = (a.size, a.size)
+    cells = a.size * a.size
+    T = a.time_steps
+    states = riemann_states(SEED, 2)
+    s = SplitSolver(shape, dtype=a.dtype, flux=a.flux, limiter="vanleer", gamma=GAMMA)
+    buf_a = s.new_state()
+    buf_b = s.new_state()
+    sim = Simulation(s)
+    stream = torch.cuda.current_stream()
+
+    def one_run(events=None):
+        s.fill_riemann(states, out=buf_a)
+        sim.begin(buf_a, buf_b, 0.8, 1.0 / a.size, 1e30, T)
+        if events is not None:
+            events[0].record(stream)
+        sim.steps(T)
+        if events is not None:
+            events[1].record(stream)
+
+    for _ in range(a.warmup):
+        one_run()
+    it, _, done, _ = sim.status()
+    if it != T:
+        raise RuntimeError(f"warm-up run stopped after {it} of {T} steps (non-finite state?)")
+
+    sampler = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(a.steps):
+        one_run(ev[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    sweep_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    it, _, done, _ = sim.status()
+    if it != T:
+        raise RuntimeError(f"timed run stopped after {it} of {T} steps")
+    elapsed_ms = max_over_ranks(elapsed_ms, world, dev)
+
+    elem = 8 if a.dtype == "f64" else 4
+    nc = 4
+    launches_per_run = 2 * T
+    sweep_s = sweep_ms / 1e3 / (a.steps * launches_per_run)
+    bytes_per_sweep = 2 * nc * elem * cells          # one read + one write of the state
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = bytes_per_sweep / sweep_s / 1e9
+    value = world * cells * T * a.steps / (elapsed_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    pinned_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
+    pinned_out = torch.empty_like(pinned_in)
+    s.fill_riemann(states, out=buf_a)
+    pinned_in.copy_(buf_a)
+    torch.cuda.synchronize()
+    e2e_steps = max(2, min(a.steps, 5))
+
+    def e2e_run():
+        buf_a.copy_(pinned_in, non_blocking=True)
+        res, it2, _ = sim.run(buf_a, buf_b, 0.8, 1.0 / a.size, 1e30, T)
+        pinned_out.copy_(res, non_blocking=True)
+        torch.cuda.synchronize()
+        return it2
+
+    e2e_run()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        it2 = e2e_run()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, world, dev)
+    if it2 != T:
+        raise RuntimeError("end-to-end run did not complete")
+    e2e_value = world * cells * T * e2e_steps / e2e_s
+    state_bytes = nc * elem * cells
+
+    variants = {}
+    if not a.no_variants and rank == 0:
+        for dt_, fx in (("f32", "hllc"), ("f64", "force"), ("f32", "force")):
+            if (dt_, fx) == (a.dtype, a.flux):
+                continue
+            variants[f"{fx}_{dt_}"] = measure_variant(a, dt_, fx, states)
+
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
+        "config": workload_config(a),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "sweep_kernel (x and y sweeps, averaged)",
+                     "algorithmic_bytes_per_launch": bytes_per_sweep,
+                     "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": a.steps * (3 + launches_per_run),
+        "clocks": clocks,
+    }
+    if variants:
+        line["variants"] = variants
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference_rate(a)
+        line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores,
+                                "kind": kind, "sample": sample}
+    if rank == 0:
+        print(json.dumps(line))
+    del sim
+
+
+def measure_variant(a, dtype, flux, states, runs=3):
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    s = SplitSolver((a.size, a.size), dtype=dtype, flux=flux, gamma=GAMMA)
+    x = s.new_state()
+    y = s.new_state()
+    sim = Simulation(s)
+    T = a.time_steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for k in range(runs + 1):
+        s.fill_riemann(states, out=x)
+        sim.begin(x, y, 0.8, 1.0 / a.size, 1e30, T)
+        e0.record()
+        sim.steps(T)
+        e1.record()
+        torch.cuda.synchronize()
+        if k > 0:
+            total += e0.elapsed_time(e1)
+    it, _, _, _ = sim.status()
+    elem = 8 if dtype == "f64" else 4
+    sweep_s = total / 1e3 / (runs * 2 * T)
+    cells = a.size * a.size
+    return {"cell_updates_per_s": cells * T * runs / (total / 1e3),
+            "sweep_gbs": 2 * 4 * elem * cells / sweep_s / 1e9, "steps_completed": it}
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_init(a)
+    try:
+        if a.impl == "reference":
+            run_reference_arm(a, world, rank)
+        else:
+            run_ours(a, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

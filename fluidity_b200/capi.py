@@ -1,0 +1,120 @@
+"""ctypes binding of the C ABI declared in include/fluidity_b200.h.
+
+The library is built in-tree (fluidity_b200/libfluidity_b200.so).  Loading
+fails loudly when it is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfluidity_b200.so")
+
+FL_OK, FL_EINVAL, FL_ECUDA, FL_ETIMEOUT, FL_ENAN, FL_ENOMEM = 0, 1, 2, 3, 4, 5
+
+FL_DTYPE_F64 = 0
+FL_DTYPE_F32 = 1
+FL_FLUX_HLLC = 0 << 1
+FL_FLUX_FORCE = 1 << 1
+FL_FLUX_LF = 2 << 1
+FL_FLUX_RICHTMYER = 3 << 1
+FL_LIMITER_VANLEER = 0 << 3
+FL_LIMITER_SUPERBEE = 1 << 3
+FL_RECON_MUSCL = 0 << 4
+FL_RECON_BASIC = 1 << 4
+FL_NO_FLATTEN = 1 << 5
+
+FLUX_BITS = {"hllc": FL_FLUX_HLLC, "force": FL_FLUX_FORCE, "lf": FL_FLUX_LF,
+             "richtmyer": FL_FLUX_RICHTMYER}
+LIMITER_BITS = {"vanleer": FL_LIMITER_VANLEER, "superbee": FL_LIMITER_SUPERBEE}
+RECON_BITS = {"muscl": FL_RECON_MUSCL, "basic": FL_RECON_BASIC}
+
+
+class FlError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[fl status {code}] {message}")
+        self.code = code
+
+
+class Grid(C.Structure):
+    _fields_ = [("dims", C.c_int32), ("n", C.c_int64 * 3), ("pitch", C.c_int64)]
+
+    @staticmethod
+    def make(shape, pitch: int | None = None) -> "Grid":
+        """shape = (nx,), (nx, ny) or (nx, ny, nz), x first."""
+        g = Grid()
+        g.dims = len(shape)
+        n = list(shape) + [1] * (3 - len(shape))
+        for d in range(3):
+            g.n[d] = int(n[d])
+        cells = 1
+        for v in shape:
+            cells *= int(v)
+        g.pitch = int(pitch if pitch is not None else cells)
+        return g
+
+
+def policy_bits(dtype: str = "f64", flux: str = "hllc", limiter: str = "vanleer",
+                recon: str = "muscl", flatten: bool = True) -> int:
+    bits = FL_DTYPE_F32 if dtype in ("f32", "float32", "float") else FL_DTYPE_F64
+    bits |= FLUX_BITS[flux] | LIMITER_BITS[limiter] | RECON_BITS[recon]
+    if not flatten:
+        bits |= FL_NO_FLATTEN
+    return bits
+
+
+# name -> (restype, argtypes); every symbol of include/fluidity_b200.h
+_P = C.c_void_p
+_G = C.POINTER(Grid)
+PROTOTYPES = {
+    "fl_version": (C.c_int, []),
+    "fl_last_error_string": (C.c_char_p, []),
+    "fl_state_bytes": (C.c_int64, [_G, C.c_uint32]),
+    "fl_split_sweep": (C.c_int, [_G, C.c_int, _P, _P, C.c_double, C.c_double, C.c_uint32,
+                                 C.c_uint32, _P, _P]),
+    "fl_split_solve": (C.c_int, [_G, C.POINTER(_P), C.POINTER(_P), C.c_double, C.c_double,
+                                 C.c_uint32, C.c_uint32, _P, _P]),
+    "fl_max_wavespeed": (C.c_int, [_G, _P, C.c_double, C.c_uint32, _P, _P]),
+    "fl_fill_riemann": (C.c_int, [_G, _P, C.c_double, C.c_uint32, _P, _P]),
+    "fl_aos_to_soa": (C.c_int, [_G, C.c_uint32, _P, _P, _P]),
+    "fl_soa_to_aos": (C.c_int, [_G, C.c_uint32, _P, _P, _P]),
+    "fl_sim_create": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32]),
+    "fl_sim_destroy": (C.c_int, [_P]),
+    "fl_sim_begin": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P]),
+    "fl_sim_steps": (C.c_int, [_P, C.c_int64, _P]),
+    "fl_sim_status": (C.c_int, [_P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int), C.POINTER(_P)]),
+    "fl_simulate": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P,
+                              C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(_P)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (built by fluidity_b200.build); raise if absent."""
+    global _lib
+    if _lib is not None and path == LIB_PATH:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python -m fluidity_b200.build` "
+            "(the split solver has no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path == LIB_PATH:
+        _lib = lib
+    return lib
+
+
+def check(rc: int, lib=None) -> None:
+    if rc != FL_OK:
+        lib = lib or load()
+        msg = lib.fl_last_error_string().decode(errors="replace")
+        raise FlError(rc, msg)

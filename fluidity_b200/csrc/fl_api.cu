@@ -1,0 +1,504 @@
+// fl_api.cu -- C ABI of the split-solver step (include/fluidity_b200.h):
+// argument checking, status codes, the wavespeed / fill / layout kernels and
+// the device-resident time loop.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/fluidity_b200.h"
+#include "fl_internal.cuh"
+#include "fl_launch.cuh"
+#include "fl_numerics.cuh"
+#include "fl_sweep.cuh"
+
+namespace fl {
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+  return kECuda;
+}
+
+struct Policy {
+  bool f32;
+  int flux;
+  int limiter;
+  int basic;
+  int flatten;
+};
+
+Policy decode(uint32_t policy) {
+  Policy p;
+  p.f32 = (policy & 1u) != 0;
+  p.flux = (int)((policy >> 1) & 3u);
+  p.limiter = (int)((policy >> 3) & 1u);
+  p.basic = (int)((policy >> 4) & 1u);
+  p.flatten = ((policy >> 5) & 1u) ? 0 : 1;
+  return p;
+}
+
+int check_grid(const fl_grid* g) {
+  if (g == nullptr) return fail(kEInval, "grid is NULL");
+  if (g->dims < 1 || g->dims > 3) return fail(kEInval, "dims must be 1..3 (got %d)", (int)g->dims);
+  int64_t cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (d < g->dims) {
+      if (g->n[d] < 4)
+        return fail(kEInval, "n[%d] must be >= 4 (got %lld)", d, (long long)g->n[d]);
+    } else if (g->n[d] != 1) {
+      return fail(kEInval, "n[%d] must be 1 beyond dims (got %lld)", d, (long long)g->n[d]);
+    }
+    cells *= g->n[d];
+  }
+  if (g->pitch < cells) return fail(kEInval, "pitch %lld smaller than the cell count %lld", (long long)g->pitch, (long long)cells);
+  if ((uint64_t)g->n[1] > 65535ull * 64 || (uint64_t)g->n[2] > 65535ull * 4)
+    return fail(kEInval, "grid too large in y or z");
+  return kOk;
+}
+
+int check_policy(uint32_t policy) {
+  if (policy & ~0x3fu) return fail(kEInval, "unknown policy bits (0x%x)", (unsigned)policy);
+  return kOk;
+}
+
+size_t elem_size(const Policy& p) { return p.f32 ? sizeof(float) : sizeof(double); }
+
+SweepParams make_params(const fl_grid* g, const Policy& pol, double gamma, double dtdh,
+                        uint32_t boundary) {
+  SweepParams p;
+  memset(&p, 0, sizeof(p));
+  p.pitch = g->pitch;
+  for (int d = 0; d < 3; ++d) p.n[d] = g->n[d];
+  p.gamma = gamma;
+  p.dtdh = dtdh;
+  p.limiter = pol.limiter;
+  p.basic = pol.basic;
+  p.flatten = pol.flatten;
+  p.reflect = boundary;
+  return p;
+}
+
+cudaError_t launch_sweep(const SweepParams& p, const Policy& pol, int dims, int dim,
+                         cudaStream_t st) {
+  return pol.f32 ? launch_sweep_f32(p, dims, dim, pol.flux, st)
+                 : launch_sweep_f64(p, dims, dim, pol.flux, st);
+}
+
+// ---- wavespeed reduction (set_wavespeeds + max_element) -----------------
+
+template <typename T, int D>
+__global__ void __launch_bounds__(256) wavespeed_kernel(const T* __restrict__ in, int64_t pitch,
+                                                        int64_t cells, T gamma,
+                                                        unsigned long long* accum,
+                                                        StepControl* ctrl) {
+  __shared__ double s_red[8];
+  double local = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Cons<T, D> u;
+#pragma unroll
+    for (int c = 0; c < D + 2; ++c) u.v[c] = __ldg(in + c * pitch + i);
+    ws_max(local, (double)max_wavespeed(u, gamma));
+  }
+  cta_wavespeed_commit<256>(local, accum, ctrl, ctrl != nullptr ? 1 : 0, false, s_red);
+}
+
+template <typename T>
+cudaError_t launch_wavespeed(const fl_grid* g, const void* in, double gamma,
+                             unsigned long long* accum, StepControl* ctrl, cudaStream_t st) {
+  const int64_t cells = g->n[0] * g->n[1] * g->n[2];
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t blocks = (cells + 255) / 256;
+  if (blocks > (int64_t)sms * 8) blocks = (int64_t)sms * 8;
+  if (blocks < 1) blocks = 1;
+  const T* p = static_cast<const T*>(in);
+  switch (g->dims) {
+    case 1: wavespeed_kernel<T, 1><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
+    case 2: wavespeed_kernel<T, 2><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
+    default: wavespeed_kernel<T, 3><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
+  }
+  return cudaGetLastError();
+}
+
+// ---- initial state -------------------------------------------------------
+
+template <typename T>
+struct RiemannStates {
+  T s[8][5];
+};
+
+template <typename T>
+__global__ void fill_riemann_kernel(T* __restrict__ out, int64_t pitch, int64_t n0, int64_t n1,
+                                    int64_t n2, int dims, RiemannStates<T> st) {
+  const int64_t cells = n0 * n1 * n2;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c[3] = {i % n0, (i / n0) % n1, i / (n0 * n1)};
+    const int64_t n[3] = {n0, n1, n2};
+    int s = 0;
+    for (int d = 0; d < dims; ++d) {
+      // pos[d] = float(i_d) / N_d in float (simulator_impl.hpp:324)
+      const float pos = __fdiv_rn((float)c[d], (float)n[d]);
+      if (!((double)pos < 0.5)) s |= 1 << d;
+    }
+    for (int k = 0; k < dims + 2; ++k) out[k * pitch + i] = st.s[s][k];
+  }
+}
+
+template <typename T>
+void prim_to_cons_host(int D, const double* prim_d, T gamma, T* cons) {
+  // state_impl.hpp:390-406 (energy 136-142, eos ideal_gas.hpp:59-63)
+  T prim[5];
+  for (int k = 0; k < D + 2; ++k) prim[k] = (T)prim_d[k];
+  // host code is compiled with -ffp-contract=off: every product is rounded
+  T v2 = T(0);
+  for (int d = 0; d < D; ++d) v2 += prim[2 + d] * prim[2 + d];
+  const T e = prim[1] / ((gamma - T(1)) * prim[0]);
+  cons[0] = prim[0];
+  cons[1] = prim[0] * (T(0.5) * v2 + e);
+  for (int d = 0; d < D; ++d) cons[2 + d] = prim[2 + d] * prim[0];
+}
+
+template <typename T>
+cudaError_t launch_fill(const fl_grid* g, const double* states, double gamma, void* out,
+                        cudaStream_t st) {
+  RiemannStates<T> rs;
+  memset(&rs, 0, sizeof(rs));
+  const int D = g->dims;
+  for (int s = 0; s < (1 << D); ++s) prim_to_cons_host<T>(D, states + s * (D + 2), (T)gamma, rs.s[s]);
+  const int64_t cells = g->n[0] * g->n[1] * g->n[2];
+  int64_t blocks = (cells + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  fill_riemann_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(static_cast<T*>(out), g->pitch, g->n[0],
+                                                           g->n[1], g->n[2], D, rs);
+  return cudaGetLastError();
+}
+
+// ---- AoS <-> SoA -----------------------------------------------------------
+
+template <typename T>
+__global__ void aos_soa_kernel(const T* __restrict__ src, T* __restrict__ dst, int64_t cells,
+                               int nc, int64_t pitch, int to_soa) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells * nc;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (to_soa) {
+      const int64_t cell = i / nc, c = i % nc;
+      dst[c * pitch + cell] = src[i];
+    } else {
+      const int64_t cell = i / nc, c = i % nc;
+      dst[i] = src[c * pitch + cell];
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_layout(const fl_grid* g, const void* src, void* dst, int to_soa,
+                          cudaStream_t st) {
+  const int64_t cells = g->n[0] * g->n[1] * g->n[2];
+  int64_t blocks = (cells * (g->dims + 2) + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  aos_soa_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(static_cast<const T*>(src),
+                                                      static_cast<T*>(dst), cells, g->dims + 2,
+                                                      g->pitch, to_soa);
+  return cudaGetLastError();
+}
+
+// ---- time control ----------------------------------------------------------
+
+__global__ void init_control_kernel(StepControl* c, double cfl, double res, double sim_time,
+                                    long long max_iters, int is_f32) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    c->dt = 0.0;
+    c->dtdh = 0.0;
+    c->run_time = 0.0;
+    c->sim_time = is_f32 ? (double)(float)sim_time : sim_time;
+    c->cfl = is_f32 ? (double)(float)cfl : cfl;
+    c->res = res;
+    c->iters = 0;
+    c->max_iters = max_iters;
+    c->ws_bits = 0ull;
+    c->arrive = 0u;
+    c->done = 0;
+    c->is_f32 = is_f32;
+    c->status = 0;
+  }
+}
+
+}  // namespace
+}  // namespace fl
+
+struct fl_sim {
+  fl_grid grid;
+  fl::Policy pol;
+  uint32_t policy;
+  double gamma;
+  uint32_t boundary;
+  int device;
+  fl::StepControl* ctrl;   // device
+  void* a;
+  void* b;
+  int64_t enqueued;        // steps enqueued since fl_sim_begin
+};
+
+using namespace fl;
+
+extern "C" {
+
+int fl_version(void) { return 100; }
+
+const char* fl_last_error_string(void) { return g_err; }
+
+int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy) {
+  if (check_grid(grid) != kOk) return -1;
+  return (int64_t)(grid->dims + 2) * grid->pitch * (int64_t)elem_size(decode(policy));
+}
+
+int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out, double gamma,
+                   double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,
+                   void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if (dim < 0 || dim >= grid->dims) return fail(kEInval, "dim %d out of range", dim);
+  if (in == nullptr || out == nullptr) return fail(kEInval, "NULL state buffer");
+  if (in == out) return fail(kEInval, "in and out must differ");
+  if (!(gamma > 1.0)) return fail(kEInval, "gamma must exceed 1");
+  if (boundary_mask >> grid->dims) return fail(kEInval, "boundary_mask has bits beyond dims");
+  const Policy pol = decode(policy);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SweepParams p = make_params(grid, pol, gamma, dtdh, boundary_mask);
+  p.in = in;
+  p.out = out;
+  if (max_ws_out != nullptr) {
+    cudaError_t e = cudaMemsetAsync(max_ws_out, 0, sizeof(double), st);
+    if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
+    p.ws_accum = reinterpret_cast<unsigned long long*>(max_ws_out);
+  }
+  cudaError_t e = launch_sweep(p, pol, grid->dims, dim, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
+  return kOk;
+}
+
+int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma, double dtdh,
+                   uint32_t policy, uint32_t boundary_mask, double* max_ws_out, void* stream) {
+  if (in == nullptr || out == nullptr) return fail(kEInval, "NULL buffer handle");
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  // split_solver.cuh:67-79: sweep x, y, z; swap between sweeps
+  for (int d = 0; d < grid->dims; ++d) {
+    double* ws = (d == grid->dims - 1) ? max_ws_out : nullptr;
+    rc = fl_split_sweep(grid, d, *in, *out, gamma, dtdh, policy, boundary_mask, ws, stream);
+    if (rc) return rc;
+    if (grid->dims != 1 && d < grid->dims - 1) {
+      void* t = *in;
+      *in = *out;
+      *out = t;
+    }
+  }
+  return kOk;
+}
+
+int fl_max_wavespeed(const fl_grid* grid, const void* in, double gamma, uint32_t policy,
+                     double* max_ws_out, void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if (in == nullptr || max_ws_out == nullptr) return fail(kEInval, "NULL pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(max_ws_out, 0, sizeof(double), st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_max_wavespeed");
+  auto* acc = reinterpret_cast<unsigned long long*>(max_ws_out);
+  e = decode(policy).f32 ? launch_wavespeed<float>(grid, in, gamma, acc, nullptr, st)
+                         : launch_wavespeed<double>(grid, in, gamma, acc, nullptr, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_max_wavespeed");
+  return kOk;
+}
+
+int fl_fill_riemann(const fl_grid* grid, const double* states_prim, double gamma,
+                    uint32_t policy, void* out, void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if (states_prim == nullptr || out == nullptr) return fail(kEInval, "NULL pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = decode(policy).f32 ? launch_fill<float>(grid, states_prim, gamma, out, st)
+                                     : launch_fill<double>(grid, states_prim, gamma, out, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_fill_riemann");
+  return kOk;
+}
+
+int fl_aos_to_soa(const fl_grid* grid, uint32_t policy, const void* aos, void* soa,
+                  void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if (aos == nullptr || soa == nullptr) return fail(kEInval, "NULL pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = decode(policy).f32 ? launch_layout<float>(grid, aos, soa, 1, st)
+                                     : launch_layout<double>(grid, aos, soa, 1, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_aos_to_soa");
+  return kOk;
+}
+
+int fl_soa_to_aos(const fl_grid* grid, uint32_t policy, const void* soa, void* aos,
+                  void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if (aos == nullptr || soa == nullptr) return fail(kEInval, "NULL pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = decode(policy).f32 ? launch_layout<float>(grid, soa, aos, 0, st)
+                                     : launch_layout<double>(grid, soa, aos, 0, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_soa_to_aos");
+  return kOk;
+}
+
+int fl_sim_create(fl_sim** sim, const fl_grid* grid, double gamma, uint32_t policy,
+                  uint32_t boundary_mask) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  *sim = nullptr;
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if (!(gamma > 1.0)) return fail(kEInval, "gamma must exceed 1");
+  if (boundary_mask >> grid->dims) return fail(kEInval, "boundary_mask has bits beyond dims");
+  fl_sim* s = new (std::nothrow) fl_sim;
+  if (s == nullptr) return fail(kENoMem, "out of host memory");
+  memset(s, 0, sizeof(*s));
+  s->grid = *grid;
+  s->pol = decode(policy);
+  s->policy = policy;
+  s->gamma = gamma;
+  s->boundary = boundary_mask;
+  cudaGetDevice(&s->device);
+  cudaError_t e = cudaMalloc(&s->ctrl, sizeof(StepControl));
+  if (e != cudaSuccess) {
+    delete s;
+    return fail(kENoMem, "cudaMalloc of the control block failed: %s", cudaGetErrorString(e));
+  }
+  e = cudaMemset(s->ctrl, 0, sizeof(StepControl));
+  if (e != cudaSuccess) {
+    cudaFree(s->ctrl);
+    delete s;
+    return cuda_fail(e, "fl_sim_create");
+  }
+  *sim = s;
+  return kOk;
+}
+
+int fl_sim_destroy(fl_sim* sim) {
+  if (sim == nullptr) return kOk;
+  cudaError_t e = cudaFree(sim->ctrl);
+  delete sim;
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_destroy");
+  return kOk;
+}
+
+int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res, double sim_time,
+                 int64_t max_iters, void* stream) {
+  if (sim == nullptr || a == nullptr || b == nullptr || a == b)
+    return fail(kEInval, "invalid sim or buffers");
+  if (!(cfl > 0.0) || !(res > 0.0) || max_iters < 0)
+    return fail(kEInval, "cfl and res must be positive, max_iters >= 0");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  sim->a = a;
+  sim->b = b;
+  sim->enqueued = 0;
+  init_control_kernel<<<1, 32, 0, st>>>(sim->ctrl, cfl, res, sim_time, (long long)max_iters,
+                                        sim->pol.f32 ? 1 : 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
+  auto* acc = &sim->ctrl->ws_bits;
+  e = sim->pol.f32 ? launch_wavespeed<float>(&sim->grid, a, sim->gamma, acc, sim->ctrl, st)
+                   : launch_wavespeed<double>(&sim->grid, a, sim->gamma, acc, sim->ctrl, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
+  return kOk;
+}
+
+int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
+  if (sim == nullptr || sim->a == nullptr) return fail(kEInval, "fl_sim_begin not called");
+  if (nsteps < 0) return fail(kEInval, "nsteps < 0");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int D = sim->grid.dims;
+  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, 0.0, sim->boundary);
+  p.ctrl = sim->ctrl;
+  for (int64_t k = 0; k < nsteps; ++k) {
+    // input of this step: for even D the state returns to buffer a every
+    // step; for odd D it alternates a, b, a, ...
+    const bool from_b = (D % 2 == 1) && ((sim->enqueued & 1) == 1);
+    void* si = from_b ? sim->b : sim->a;
+    void* so = from_b ? sim->a : sim->b;
+    for (int d = 0; d < D; ++d) {
+      p.in = si;
+      p.out = so;
+      const bool last = (d == D - 1);
+      p.ws_accum = last ? &sim->ctrl->ws_bits : nullptr;
+      p.finalize = last ? 1 : 0;
+      cudaError_t e = launch_sweep(p, sim->pol, D, d, st);
+      if (e != cudaSuccess) return cuda_fail(e, "fl_sim_steps");
+      if (D != 1 && d < D - 1) {
+        void* t = si;
+        si = so;
+        so = t;
+      }
+    }
+    sim->enqueued += 1;
+  }
+  return kOk;
+}
+
+int fl_sim_status(fl_sim* sim, void* stream, int64_t* iters, double* run_time, int* done,
+                  void** result) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  StepControl h;
+  cudaError_t e = cudaMemcpyAsync(&h, sim->ctrl, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_status");
+  if (iters) *iters = h.iters;
+  if (run_time) *run_time = h.run_time;
+  if (done) *done = h.done;
+  if (result) {
+    const bool in_b = (sim->grid.dims % 2 == 1) && (h.iters & 1);
+    *result = in_b ? sim->b : sim->a;
+  }
+  if (h.status == kENan) return fail(kENan, "non-finite wavespeed after step %lld", (long long)h.iters);
+  return kOk;
+}
+
+int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res, double sim_time,
+                int64_t max_iters, void* stream, int64_t* iters, double* run_time,
+                void** result) {
+  int rc = fl_sim_begin(sim, a, b, cfl, res, sim_time, max_iters, stream);
+  if (rc) return rc;
+  int done = 0;
+  int64_t it = 0;
+  while (true) {
+    rc = fl_sim_status(sim, stream, &it, run_time, &done, result);
+    if (rc) return rc;
+    if (done) break;
+    const int64_t left = max_iters - sim->enqueued;
+    const int64_t chunk = left < 64 ? left : 64;
+    if (chunk <= 0) break;
+    rc = fl_sim_steps(sim, chunk, stream);
+    if (rc) return rc;
+  }
+  if (iters) *iters = it;
+  return kOk;
+}
+
+}  // extern "C"

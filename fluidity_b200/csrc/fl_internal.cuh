@@ -1,0 +1,58 @@
+// fl_internal.cuh -- device-side structures shared by the kernels and the
+// C-ABI layer.
+#pragma once
+
+#include <cstdint>
+
+namespace fl {
+
+// Device-resident time control of one simulation (the state of
+// sim::Parameters, simulator/parameters.hpp:27-99, kept in HBM so that a whole
+// run can be launched, or captured in a CUDA graph, without host round trips).
+// Values are stored as double; an FP32 run rounds them through float exactly
+// where the reference's Parameters<float> would.
+struct StepControl {
+  double dt;          // time step of the step in flight
+  double dtdh;        // dt / dh of the step in flight
+  double run_time;    // accumulated simulated time
+  double sim_time;    // stop when run_time >= sim_time
+  double cfl;
+  double res;         // grid spacing dh
+  long long iters;    // completed steps
+  long long max_iters;
+  unsigned long long ws_bits;  // max wavespeed (double bits) of the state being produced
+  unsigned int arrive;         // blocks of the finishing sweep that have arrived
+  int done;                    // 1 once the loop condition fails
+  int is_f32;                  // round dt, dtdh and run_time through float
+  int status;                  // 0, or FL_ENAN when a wavespeed was not finite
+  int pad_;
+};
+
+// Parameters of one dimensional sweep.
+struct SweepParams {
+  const void* in;
+  void* out;
+  int64_t pitch;          // elements between component planes
+  int64_t n[3];           // cells per dimension (x fastest); unused = 1
+  double gamma;
+  double dtdh;            // used when ctrl == nullptr
+  int limiter;            // LimiterKind
+  int basic;              // 1: piecewise-constant reconstruction
+  int flatten;            // 1: slope flattening (chi) on
+  uint32_t reflect;       // bit d: reflective ends in dimension d
+  StepControl* ctrl;      // nullable: take dtdh / done from the control block
+  unsigned long long* ws_accum;  // nullable: max wavespeed of the output (double bits)
+  int finalize;           // 1: last sweep of a step; the last block advances ctrl
+};
+
+// Status codes, mirrored by include/fluidity_b200.h.
+enum : int {
+  kOk = 0,
+  kEInval = 1,
+  kECuda = 2,
+  kETimeout = 3,
+  kENan = 4,
+  kENoMem = 5,
+};
+
+}  // namespace fl

@@ -1,0 +1,216 @@
+// fl_numerics.cuh -- per-cell arithmetic of the split-solver step.
+//
+// Each function restates one of the reference's numerics functors
+// (robclu/fluidity include/fluidity/...).  The order of every floating-point
+// operation follows the reference expression, so that a build without FMA
+// contraction (-fmad=false) reproduces the reference bit for bit and the
+// default build differs only by FMA rounding.
+//
+// States are conservative, component order [rho, E, m_x, (m_y), (m_z)]
+// (state/state.hpp:88-98).  NC = D + 2.
+#pragma once
+
+#include <cstdint>
+
+namespace fl {
+
+enum FluxKind : int { kHllc = 0, kForce = 1, kLaxFriedrichs = 2, kRichtmyer = 3 };
+enum LimiterKind : int { kVanLeer = 0, kSuperbee = 1 };
+
+template <typename T> __device__ __forceinline__ T fl_sqrt(T x);
+template <> __device__ __forceinline__ double fl_sqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float fl_sqrt<float>(float x) { return sqrtf(x); }
+template <typename T> __device__ __forceinline__ T fl_abs(T x);
+template <> __device__ __forceinline__ double fl_abs<double>(double x) { return fabs(x); }
+template <> __device__ __forceinline__ float fl_abs<float>(float x) { return fabsf(x); }
+
+// std::min / std::max as the reference's <algorithm> defines them.
+template <typename T> __device__ __forceinline__ T std_min(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T std_max(T a, T b) { return (a < b) ? b : a; }
+
+template <typename T, int D>
+struct Cons {
+  static constexpr int NC = D + 2;
+  T v[NC];
+};
+
+// velocity m_d / rho (state_impl.hpp:88-96)
+template <typename T, int D>
+__device__ __forceinline__ T velocity(const Cons<T, D>& u, int d) {
+  return u.v[2 + d] / u.v[0];
+}
+
+// (gamma - 1) (E - 0.5 rho sum_d (m_d / rho)^2) (state_impl.hpp:117-128, 49-61)
+template <typename T, int D>
+__device__ __forceinline__ T pressure(const Cons<T, D>& u, T gamma) {
+  T sum = T(0);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const T v = u.v[2 + d] / u.v[0];
+    sum += v * v;
+  }
+  return (gamma - T(1)) * (u.v[1] - T(0.5) * u.v[0] * sum);
+}
+
+// Conservative physical flux in dimension d, given its velocity and pressure
+// (state_impl.hpp:293-310, make_other_fluxes 228-244).
+template <typename T, int D>
+__device__ __forceinline__ void flux_vp(const Cons<T, D>& u, int d, T v, T p,
+                                        Cons<T, D>& f) {
+  f.v[0] = u.v[2 + d];
+  f.v[2 + d] = u.v[2 + d] * v + p;
+  f.v[1] = v * (u.v[1] + p);
+#pragma unroll
+  for (int t = 0; t < D; ++t)
+    if (t != d) f.v[2 + t] = u.v[2 + t] * v;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void flux(const Cons<T, D>& u, int d, T gamma,
+                                     Cons<T, D>& f) {
+  flux_vp(u, d, velocity(u, d), pressure(u, gamma), f);
+}
+
+// sqrt(gamma p / rho) (material/ideal_gas.hpp:75-78)
+template <typename T, int D>
+__device__ __forceinline__ T sound_speed_p(const Cons<T, D>& u, T gamma, T p) {
+  return fl_sqrt<T>(gamma * p / u.v[0]);
+}
+
+// max_d |u_d| + a (state_impl.hpp:167-178)
+template <typename T, int D>
+__device__ __forceinline__ T max_wavespeed(const Cons<T, D>& u, T gamma) {
+  T m = fl_abs<T>(velocity(u, 0));
+#pragma unroll
+  for (int d = 1; d < D; ++d) m = std_max(m, fl_abs<T>(velocity(u, d)));
+  return m + sound_speed_p(u, gamma, pressure(u, gamma));
+}
+
+// ---- HLLC (flux_method/flux_hllc.hpp:56-245) ---------------------------
+
+template <typename T, int D>
+__device__ __forceinline__ void hllc_star(const Cons<T, D>& u, int d, T s, T sstar,
+                                          T vel, T p, Cons<T, D>& out) {
+  const T sf = s - vel;
+  const T scale = sf / (s - sstar);
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c) out.v[c] = scale * u.v[c];
+  out.v[2 + d] = sstar * u.v[0] * scale;
+  out.v[1] = scale * (u.v[1] + u.v[0] * (sstar - vel) * (sstar + p / (u.v[0] * sf)));
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void hllc(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
+                                     T gamma, Cons<T, D>& f) {
+  const T pl = pressure(ul, gamma), pr = pressure(ur, gamma);
+  const T vl = velocity(ul, d), vr = velocity(ur, d);
+  const T al = sound_speed_p(ul, gamma, pl);
+  const T ar = sound_speed_p(ur, gamma, pr);
+  const T adi = (gamma + T(1)) / (T(2) * gamma);
+  const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * (vr - vl) * (ur.v[0] + ul.v[0]) * (al + ar)));
+  const T p_star = std_max(T(0), p_pvrs);
+  // wavespeed(): rarefaction if p* <= p_K, else shock (flux_hllc.hpp:81-99)
+  const T wsl = (p_star <= pl) ? vl + (-al)
+                               : vl + (-al) * fl_sqrt<T>(T(1) + adi * (p_star / pl - T(1)));
+  if (T(0) <= wsl) { flux_vp(ul, d, vl, pl, f); return; }
+  const T wsr = (p_star <= pr) ? vr + ar
+                               : vr + ar * fl_sqrt<T>(T(1) + adi * (p_star / pr - T(1)));
+  if (T(0) >= wsr) { flux_vp(ur, d, vr, pr, f); return; }
+  // star_speed (flux_hllc.hpp:113-137)
+  const T factl = ul.v[0] * (wsl - vl);
+  const T factr = ur.v[0] * (wsr - vr);
+  const T sstar = (pr - pl + vl * factl - vr * factr) / (factl - factr);
+  Cons<T, D> st;
+  if (T(0) <= sstar) {
+    flux_vp(ul, d, vl, pl, f);
+    hllc_star(ul, d, wsl, sstar, vl, pl, st);
+#pragma unroll
+    for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + wsl * (st.v[c] - ul.v[c]);
+  } else {
+    flux_vp(ur, d, vr, pr, f);
+    hllc_star(ur, d, wsr, sstar, vr, pr, st);
+#pragma unroll
+    for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + wsr * (st.v[c] - ur.v[c]);
+  }
+}
+
+// ---- FORCE = (LF + Richtmyer) / 2 (flux_force.hpp:73-84) ----------------
+
+template <typename T, int D>
+__device__ __forceinline__ void lax_friedrichs_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
+                                                  const Cons<T, D>& fl, const Cons<T, D>& fr,
+                                                  T dtdh, Cons<T, D>& f) {
+  // flux_lax_friedrichs.hpp:63-78; dhdt = 1 / dtdh
+  const T dhdt = T(1.0) / dtdh;
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c)
+    f.v[c] = T(0.5) * (fl.v[c] + fr.v[c] + dhdt * (ul.v[c] - ur.v[c]));
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void richtmyer_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
+                                             const Cons<T, D>& fl, const Cons<T, D>& fr,
+                                             int d, T gamma, T dtdh, Cons<T, D>& f) {
+  // flux_richtmyer.hpp:78-88
+  Cons<T, D> u;
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c)
+    u.v[c] = T(0.5) * (ul.v[c] + ur.v[c] + dtdh * (fl.v[c] - fr.v[c]));
+  flux(u, d, gamma, f);
+}
+
+template <int FLUX, typename T, int D>
+__device__ __forceinline__ void riemann(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
+                                        T gamma, T dtdh, Cons<T, D>& f) {
+  if constexpr (FLUX == kHllc) {
+    hllc(ul, ur, d, gamma, f);
+  } else {
+    Cons<T, D> fl, fr;
+    flux(ul, d, gamma, fl);
+    flux(ur, d, gamma, fr);
+    if constexpr (FLUX == kLaxFriedrichs) {
+      lax_friedrichs_ff(ul, ur, fl, fr, dtdh, f);
+    } else if constexpr (FLUX == kRichtmyer) {
+      richtmyer_ff(ul, ur, fl, fr, d, gamma, dtdh, f);
+    } else {
+      Cons<T, D> a, b;
+      lax_friedrichs_ff(ul, ur, fl, fr, dtdh, a);
+      richtmyer_ff(ul, ur, fl, fr, d, gamma, dtdh, b);
+#pragma unroll
+      for (int c = 0; c < D + 2; ++c) f.v[c] = T(0.5) * (a.v[c] + b.v[c]);
+    }
+  }
+}
+
+// ---- limiters (limiting/van_leer_limiter.hpp:65-74, superbee 72-89) -----
+
+template <typename T>
+__device__ __forceinline__ T limit_single(int limiter, T left, T right) {
+  const T r = left / right;
+  if (limiter == kSuperbee) {
+    if (r <= T(0) || right == T(0)) return T(0);
+    if (r <= T(0.5)) return T(2) * r;
+    if (r <= T(1)) return T(1);
+    const T er = T(2) / (T(1) + r);
+    return std_min(er, std_min(r, T(2)));
+  }
+  return (r <= T(0) || right == T(0)) ? T(0) : T(2) * std_min(r, T(1)) / (T(1) + r);
+}
+
+// ---- flattening (reconstruction/muscl_reconstructor.hpp:59-87) ----------
+// Inputs: pressures at c+1, c-1, c+2, c-2 and velocities (sweep of chi's own
+// dimension) at c-1, c+1.  Ratio in T; sigma test and eta in double.
+
+template <typename T>
+__device__ __forceinline__ double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
+                                           T u_prev, T u_next) {
+  const T u_factor = u_prev - u_next;
+  const T dp = fl_abs<T>(p_next - p_prev);
+  const bool flatten = ((double)u_factor > 0.0) && ((double)(dp / std_min(p_next, p_prev)) > 0.33);
+  if (!flatten) return 1.0;
+  const T z = dp / fl_abs<T>(p_nnext - p_pprev);
+  const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
+  return std_min(1.0, std_max(0.0, temp));
+}
+
+}  // namespace fl

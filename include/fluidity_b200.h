@@ -1,0 +1,155 @@
+/*
+ * fluidity_b200.h -- C ABI of the B200-native split-solver step.
+ *
+ * Drop-in boundary for robclu/fluidity's finite-volume Euler hot path.  Each
+ * entry point names the reference interface it replaces (paths relative to
+ * the reference's include/fluidity/).  All device buffers belong to the
+ * caller; no entry point that launches work allocates memory, except
+ * fl_sim_create, which allocates one small control block.
+ *
+ * Storage.  The reference stores AoS states in a DeviceTensor
+ * (container/device_tensor.hpp:34-316).  This library works on
+ * structure-of-arrays component planes: component c (order
+ * [rho, E, m_x, m_y, m_z], state/state.hpp:88-98) of cell (x, y, z) lives at
+ *     base[c * pitch + (z * n[1] + y) * n[0] + x]        (x fastest)
+ * fl_aos_to_soa / fl_soa_to_aos convert from and to the reference layout.
+ *
+ * Errors.  Every call returns an FL_* status and never terminates the process
+ * (the reference prints and calls std::terminate, utility/debug.hpp:42-50).
+ * fl_last_error_string() describes the last failure on the calling thread.
+ *
+ * Streams.  Work is enqueued on the given cudaStream_t (passed as void*;
+ * NULL = legacy default stream) with no implicit device synchronisation,
+ * except in fl_sim_status / fl_simulate, which wait for the stream.
+ */
+#ifndef FLUIDITY_B200_H
+#define FLUIDITY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace fluidity_check_cuda_result, utility/debug.hpp:42-67) */
+#define FL_OK        0
+#define FL_EINVAL    1   /* invalid argument (sizes, pointers, policy)        */
+#define FL_ECUDA     2   /* a CUDA runtime call failed                        */
+#define FL_ETIMEOUT  3   /* a bounded wait gave up                            */
+#define FL_ENAN      4   /* a wavespeed was not finite (state blew up)        */
+#define FL_ENOMEM    5   /* fl_sim_create could not allocate its control      */
+
+/* ---- policy bits: the reference's compile-time policy list
+ * SimulatorImpl<data_t, Num<D>, Material, LimitForm, Limiter, Recon, Flux, ...>
+ * (simulator/simulator_traits.hpp:41-84), as run-time bits. */
+#define FL_DTYPE_F64        0u          /* data_t = double                       */
+#define FL_DTYPE_F32        1u          /* data_t = float                        */
+#define FL_FLUX_HLLC        (0u << 1)   /* flux::Hllc (flux_method/flux_hllc.hpp)  */
+#define FL_FLUX_FORCE       (1u << 1)   /* flux::Force (flux_force.hpp)            */
+#define FL_FLUX_LF          (2u << 1)   /* flux::LaxFriedrichs                     */
+#define FL_FLUX_RICHTMYER   (3u << 1)   /* flux::Richtmyer                         */
+#define FL_LIMITER_VANLEER  (0u << 3)   /* limit::VanLeer<cons_form_t>             */
+#define FL_LIMITER_SUPERBEE (1u << 3)   /* limit::Superbee<cons_form_t>            */
+#define FL_RECON_MUSCL      (0u << 4)   /* recon::MHReconstructor<Limiter>         */
+#define FL_RECON_BASIC      (1u << 4)   /* recon::BasicReconstructor               */
+#define FL_NO_FLATTEN       (1u << 5)   /* drop MUSCL's pressure flattening (chi); */
+                                        /* not a reference option                  */
+
+/* Grid description.  dims in 1..3, n[d] >= 4 for d < dims (mirror ghosts
+ * reach 4 cells deep), n[d] = 1 for d >= dims, pitch >= n[0]*n[1]*n[2]. */
+typedef struct fl_grid {
+  int32_t dims;
+  int64_t n[3];
+  int64_t pitch;
+} fl_grid;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int fl_version(void);
+
+/* Description of the last failure on the calling thread ("" if none). */
+const char* fl_last_error_string(void);
+
+/* Number of bytes of one state buffer: (dims + 2) * pitch * sizeof(T). */
+int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy);
+
+/* One dimensional sweep: out = in + dtdh * (F(i-1/2) - F(i+1/2)) along dim,
+ * ghosts per boundary_mask (bit d set = reflective ends in dimension d,
+ * transmissive otherwise; both ends of a dimension share one setting as in
+ * BoundarySetter::bit_index, solver/boundary_loader.hpp:105-111).
+ * Replaces solve_dim<SplitSolver> (solver/cuda/split_solver.cuh:39-44) and
+ * SplitSolver::invoke (solver/split_solver.hpp:138-162).
+ * max_ws_out (nullable, device pointer) receives the maximum wavespeed
+ * max_d |u_d| + a of the OUTPUT state -- the fused form of set_wavespeeds +
+ * max_element (simulator/cuda/wavespeed_initialization.cuh:85-97,
+ * algorithm/max_element.hpp:28-38) for the next step. */
+int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out,
+                   double gamma, double dtdh, uint32_t policy,
+                   uint32_t boundary_mask, double* max_ws_out, void* stream);
+
+/* All dims sweeps of one step, x then y then z, with the reference's buffer
+ * swap: replaces SplitSolver::solve (solver/split_solver.hpp:105-115) and
+ * solve_impl_split (solver/cuda/split_solver.cuh:57-80).  On return *out
+ * points at the buffer holding the new state and *in at the other one, just
+ * as the reference swaps its iterators.  max_ws_out as for fl_split_sweep. */
+int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma,
+                   double dtdh, uint32_t policy, uint32_t boundary_mask,
+                   double* max_ws_out, void* stream);
+
+/* Max over cells of max_d |u_d| + a, written to *max_ws_out (device
+ * pointer).  Replaces set_wavespeeds + max_element
+ * (simulator/cuda/wavespeed_initialization.cuh:41-97, algorithm/reduce.cuh
+ * :44-131) without the per-cell wavespeed buffer or the host-side finish. */
+int fl_max_wavespeed(const fl_grid* grid, const void* in, double gamma,
+                     uint32_t policy, double* max_ws_out, void* stream);
+
+/* Piecewise-constant initial state (SimulatorImpl::fill_data,
+ * simulator/simulator_impl.hpp:294-340): 2^dims primitive states
+ * (rho, p, v_x, .., host memory, doubles) assigned by orthant
+ * (x_d >= 0.5) << d of the cell position float(i_d)/float(n_d), converted to
+ * conservative form in the policy's precision. */
+int fl_fill_riemann(const fl_grid* grid, const double* states_prim,
+                    double gamma, uint32_t policy, void* out, void* stream);
+
+/* Layout adapters for the reference's AoS DeviceTensor<State, D>
+ * (container/device_tensor.hpp): aos holds cells * (dims + 2) values. */
+int fl_aos_to_soa(const fl_grid* grid, uint32_t policy, const void* aos,
+                  void* soa, void* stream);
+int fl_soa_to_aos(const fl_grid* grid, uint32_t policy, const void* soa,
+                  void* aos, void* stream);
+
+/* ---- device-resident time loop: SimulatorImpl::simulate
+ * (simulator/simulator_impl.hpp:223-258) with sim::Parameters
+ * (simulator/parameters.hpp:27-99) kept in HBM.  The CFL reduction is fused
+ * into each step's last sweep; the host does not read anything back per step,
+ * so a run can be enqueued (or captured into a CUDA graph) in one go. */
+typedef struct fl_sim fl_sim;
+
+/* Allocates the control block on the current device. */
+int fl_sim_create(fl_sim** sim, const fl_grid* grid, double gamma,
+                  uint32_t policy, uint32_t boundary_mask);
+int fl_sim_destroy(fl_sim* sim);
+
+/* Resets the loop: buffers a (initial state) and b, cfl, resolution dh,
+ * stop time and step limit; enqueues the initial wavespeed reduction. */
+int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res,
+                 double sim_time, int64_t max_iters, void* stream);
+
+/* Enqueues nsteps further steps.  Steps after the loop condition fails are
+ * launched but do no work. */
+int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream);
+
+/* Waits for the stream and reports the loop state.  *result points at the
+ * buffer (a or b) holding the latest state.  Returns FL_ENAN if a wavespeed
+ * was not finite. */
+int fl_sim_status(fl_sim* sim, void* stream, int64_t* iters, double* run_time,
+                  int* done, void** result);
+
+/* Convenience: begin + steps in chunks until done, like simulate(). */
+int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res,
+                double sim_time, int64_t max_iters, void* stream,
+                int64_t* iters, double* run_time, void** result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUIDITY_B200_H */

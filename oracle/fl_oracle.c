@@ -78,19 +78,21 @@ void flo_wavespeeds_f64(const flo_grid* g, const double* in, double gamma,
 int64_t flo_simulate_f64(const flo_grid* g, double* a, double* b, double gamma,
                          double cfl, double res, double sim_time,
                          int64_t max_iters, const flo_policy* pol,
-                         int* result_in_b, double* run_time, double* dts) {
+                         int* result_in_b, double* run_time, double* dts,
+                         int64_t dts_cap) {
   if (!check_grid(g)) return -1;
   return simulate_impl_f64(g, a, b, gamma, cfl, res, sim_time, max_iters,
-                               pol, result_in_b, run_time, dts);
+                               pol, result_in_b, run_time, dts, dts_cap);
 }
 
 int64_t flo_simulate_f32(const flo_grid* g, float* a, float* b, float gamma,
                          float cfl, double res, float sim_time,
                          int64_t max_iters, const flo_policy* pol,
-                         int* result_in_b, double* run_time, double* dts) {
+                         int* result_in_b, double* run_time, double* dts,
+                         int64_t dts_cap) {
   if (!check_grid(g)) return -1;
   return simulate_impl_f32(g, a, b, gamma, cfl, res, sim_time, max_iters,
-                               pol, result_in_b, run_time, dts);
+                               pol, result_in_b, run_time, dts, dts_cap);
 }
 
 void flo_prim_to_cons_f64(int dims, const double* prim, double gamma, double* cons) {

@@ -65,16 +65,18 @@ void flo_wavespeeds_f64(const flo_grid* g, const double* in, double gamma, doubl
 /* Time loop of SimulatorImpl::simulate (simulator/simulator_impl.hpp:223-258).
  * a and b are the two state buffers; a holds the initial state.  Returns the
  * number of steps taken; *result_in_b tells which buffer holds the result and
- * *run_time the accumulated time.  dts (nullable, length max_iters) receives
- * the dt of each step. */
+ * *run_time the accumulated time.  dts (nullable) receives the dt of the
+ * first dts_cap steps. */
 int64_t flo_simulate_f64(const flo_grid* g, double* a, double* b, double gamma,
                          double cfl, double res, double sim_time,
                          int64_t max_iters, const flo_policy* pol,
-                         int* result_in_b, double* run_time, double* dts);
+                         int* result_in_b, double* run_time, double* dts,
+                         int64_t dts_cap);
 int64_t flo_simulate_f32(const flo_grid* g, float* a, float* b, float gamma,
                          float cfl, double res, float sim_time,
                          int64_t max_iters, const flo_policy* pol,
-                         int* result_in_b, double* run_time, double* dts);
+                         int* result_in_b, double* run_time, double* dts,
+                         int64_t dts_cap);
 
 /* Primitive (rho, p, v...) to conservative conversion of one state
  * (state/state_impl.hpp:390-406 with material/ideal_gas.hpp:59-63). */

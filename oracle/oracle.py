@@ -70,11 +70,11 @@ def lib():
         L.flo_wavespeeds_f64.argtypes = [P(_Grid), C.c_void_p, C.c_double, C.c_void_p]
         L.flo_simulate_f64.argtypes = [P(_Grid), C.c_void_p, C.c_void_p, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_int64,
-                                       P(_Policy), P(C.c_int), P(C.c_double), C.c_void_p]
+                                       P(_Policy), P(C.c_int), P(C.c_double), C.c_void_p, C.c_int64]
         L.flo_simulate_f64.restype = C.c_int64
         L.flo_simulate_f32.argtypes = [P(_Grid), C.c_void_p, C.c_void_p, C.c_float,
                                        C.c_float, C.c_double, C.c_float, C.c_int64,
-                                       P(_Policy), P(C.c_int), P(C.c_double), C.c_void_p]
+                                       P(_Policy), P(C.c_int), P(C.c_double), C.c_void_p, C.c_int64]
         L.flo_simulate_f32.restype = C.c_int64
         L.flo_prim_to_cons_f64.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p]
         L.flo_prim_to_cons_f32.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_void_p]
@@ -107,7 +107,7 @@ def ref():
         L.ref_simulate_f64.argtypes = [C.c_int, P(C.c_int64), C.c_int64, C.c_void_p,
                                        C.c_void_p, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_int64, C.c_int, C.c_int, C.c_int,
-                                       C.c_uint32, P(C.c_int), P(C.c_double), C.c_void_p]
+                                       C.c_uint32, P(C.c_int), P(C.c_double), C.c_void_p, C.c_int64]
         L.ref_simulate_f64.restype = C.c_int64
         _ref = L
     return _ref
@@ -177,14 +177,15 @@ def simulate(shape, u, gamma, cfl, res, sim_time, max_iters, **pol):
     b = np.empty_like(a)
     in_b = C.c_int(0)
     rt = C.c_double(0)
-    dts = np.zeros(max(int(max_iters), 1), dtype=np.float64)
+    cap = int(min(max(int(max_iters), 1), 1 << 20))
+    dts = np.zeros(cap, dtype=np.float64)
     p = _policy(**pol)
     f = lib().flo_simulate_f64 if a.dtype == np.float64 else lib().flo_simulate_f32
     steps = f(C.byref(g), _ptr(a), _ptr(b), gamma, cfl, res, sim_time, int(max_iters),
-              C.byref(p), C.byref(in_b), C.byref(rt), _ptr(dts))
+              C.byref(p), C.byref(in_b), C.byref(rt), _ptr(dts), cap)
     if steps < 0:
         raise ValueError("oracle simulate failed")
-    return (b if in_b.value else a), int(steps), rt.value, dts[:steps]
+    return (b if in_b.value else a), int(steps), rt.value, dts[:min(steps, cap)]
 
 
 def fill_riemann(shape, states_prim, gamma, dtype=np.float64):
@@ -202,7 +203,12 @@ def fill_riemann(shape, states_prim, gamma, dtype=np.float64):
 
 
 def prim_to_cons(prim, gamma, dtype=np.float64):
-    prim = np.ascontiguousarray(prim, dtype=dtype)
+    """Primitive (rho, p, v...) -> conservative; prim is (D+2,) or (D+2, n)."""
+    prim = np.asarray(prim, dtype=dtype)
+    if prim.ndim == 2:
+        cols = [prim_to_cons(prim[:, i], gamma, dtype) for i in range(prim.shape[1])]
+        return np.ascontiguousarray(np.stack(cols, axis=1))
+    prim = np.ascontiguousarray(prim)
     D = prim.shape[0] - 2
     out = np.empty_like(prim)
     if dtype == np.float64:
@@ -213,7 +219,12 @@ def prim_to_cons(prim, gamma, dtype=np.float64):
 
 
 def cons_to_prim(cons, gamma):
-    cons = np.ascontiguousarray(cons, dtype=np.float64)
+    """Conservative -> primitive; cons is (D+2,) or (D+2, n)."""
+    cons = np.asarray(cons, dtype=np.float64)
+    if cons.ndim == 2:
+        cols = [cons_to_prim(cons[:, i], gamma) for i in range(cons.shape[1])]
+        return np.ascontiguousarray(np.stack(cols, axis=1))
+    cons = np.ascontiguousarray(cons)
     out = np.empty_like(cons)
     lib().flo_cons_to_prim_f64(cons.shape[0] - 2, _ptr(cons), gamma, _ptr(out))
     return out
@@ -276,11 +287,12 @@ def ref_simulate(shape, u, gamma, cfl, res, sim_time, max_iters, flux="hllc",
     b = np.empty_like(a)
     in_b = C.c_int(0)
     rt = C.c_double(0)
-    dts = np.zeros(max(int(max_iters), 1), dtype=np.float64)
+    cap = int(min(max(int(max_iters), 1), 1 << 20))
+    dts = np.zeros(cap, dtype=np.float64)
     steps = ref().ref_simulate_f64(D, n, int(np.prod(shape)), _ptr(a), _ptr(b), gamma, cfl,
                                    res, sim_time, int(max_iters), FLUX[flux],
                                    LIMITER[limiter], RECON[recon], reflect,
-                                   C.byref(in_b), C.byref(rt), _ptr(dts))
+                                   C.byref(in_b), C.byref(rt), _ptr(dts), cap)
     if steps < 0:
         raise ValueError("reference simulate failed")
-    return (b if in_b.value else a), int(steps), rt.value, dts[:steps]
+    return (b if in_b.value else a), int(steps), rt.value, dts[:min(steps, cap)]

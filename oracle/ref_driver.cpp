@@ -254,7 +254,8 @@ int64_t ref_simulate_f64(int dims, const int64_t* n, int64_t pitch, double* a,
                          double* b, double gamma, double cfl, double res,
                          double sim_time, int64_t max_iters, int flux,
                          int limiter, int recon, uint32_t reflect,
-                         int* result_in_b, double* run_time, double* dts) {
+                         int* result_in_b, double* run_time, double* dts,
+                         int64_t dts_cap) {
   const Grid g{dims, {n[0], dims > 1 ? n[1] : 1, dims > 2 ? n[2] : 1}, pitch};
   if (!valid(g)) return -1;
   fluid::sim::Parameters<double> params(static_cast<std::size_t>(dims));
@@ -266,7 +267,7 @@ int64_t ref_simulate_f64(int dims, const int64_t* n, int64_t pitch, double* a,
   double* out = b;
   while (params.continue_simulation()) {
     params.update_time_delta(ref_max_wavespeed_f64(dims, n, pitch, in, gamma));
-    if (dts) dts[params.iters] = params.dt();
+    if (dts && static_cast<int64_t>(params.iters) < dts_cap) dts[params.iters] = params.dt();
     const double dtdh = params.dt_dh();
     double* si = in;
     double* so = out;

@@ -1,0 +1,376 @@
+"""Parity of the CUDA split-solver step (through the C ABI) with the CPU
+oracle and with the golden fixtures computed by the reference's functors.
+
+Tolerances (per cell, per step, relative with a floor of 1e-3 of the
+component's scale, see _util.rel_err): FP64 1e-12, FP32 1e-5.  The CUDA build
+contracts multiply-adds into FMA, so FP64 differs from the reference by
+rounding only; the floor keeps near-zero momenta from inflating the ratio.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+from make_golden import load  # noqa: E402
+from _util import random_prim, rel_err  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+GAMMA = 1.4
+TOL = {"f64": 1e-12, "f32": 1e-5}
+NPDT = {"f64": np.float64, "f32": np.float32}
+
+
+def to_dev(u, dtype, pitch=None):
+    import torch
+    D2, cells = u.shape
+    pitch = cells if pitch is None else pitch
+    t = torch.zeros((D2, pitch), dtype=torch.float64 if dtype == "f64" else torch.float32,
+                    device="cuda")
+    t[:, :cells] = torch.from_numpy(np.ascontiguousarray(u, dtype=NPDT[dtype]))
+    return t
+
+
+def to_host(t, cells):
+    return t[:, :cells].cpu().numpy()
+
+
+def gpu_sweep(shape, dim, u, dtdh, dtype="f64", pitch=None, want_ws=False, **pol):
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    s = SplitSolver(shape, dtype=dtype, gamma=GAMMA, pitch=pitch,
+                    flux=pol.get("flux", "hllc"), limiter=pol.get("limiter", "vanleer"),
+                    recon=pol.get("recon", "muscl"), boundary_mask=pol.get("reflect", 0),
+                    flatten=pol.get("flatten", True))
+    a = to_dev(u, dtype, s.grid.pitch)
+    b = torch.empty_like(a)
+    ws = torch.zeros(1, dtype=torch.float64, device="cuda") if want_ws else None
+    s.sweep(a, b, dim, dtdh, max_ws=ws)
+    torch.cuda.synchronize()
+    out = to_host(b, int(np.prod(shape)))
+    return (out, float(ws.item())) if want_ws else out
+
+
+# ---- golden fixtures (reference functors) ---------------------------------
+
+SWEEPS = load("sweeps.npz")
+SIMS = load("simulate.npz")
+
+
+@pytest.mark.parametrize("name", sorted(k for k in SWEEPS if "maxws" not in k))
+def test_sweep_matches_reference_golden(cuda, name):
+    c = SWEEPS[name]
+    shape = tuple(int(v) for v in c["shape"])
+    out = gpu_sweep(shape, int(c["dim"]), c["u"], c["dtdh"], flux=c["flux"],
+                    limiter=c["limiter"], recon=c["recon"], reflect=int(c["reflect"]))
+    ref = c["out"]
+    finite = np.isfinite(ref).all(axis=0)
+    # cells the reference blows up (white-noise inputs) must blow up here too
+    assert not np.isfinite(out[:, ~finite]).all(axis=0).any()
+    assert rel_err(out[:, finite], ref[:, finite]) < TOL["f64"]
+
+
+@pytest.mark.parametrize("name", sorted(k for k in SWEEPS if "maxws" in k))
+def test_max_wavespeed_matches_reference_golden(cuda, name):
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    c = SWEEPS[name]
+    shape = tuple(int(v) for v in c["shape"])
+    s = SplitSolver(shape, gamma=GAMMA)
+    ws = s.max_wavespeed(to_dev(c["u"], "f64")).item()
+    assert abs(ws - c["ws"]) <= 1e-14 * c["ws"]
+
+
+@pytest.mark.parametrize("name", sorted(SIMS))
+def test_simulate_matches_reference_golden(cuda, name):
+    """Whole device-resident runs against the reference's own loop."""
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    c = SIMS[name]
+    shape = tuple(int(v) for v in c["shape"])
+    s = SplitSolver(shape, gamma=GAMMA, flux=c["flux"], limiter=c["limiter"],
+                    recon=c["recon"], boundary_mask=int(c["reflect"]))
+    a = s.fill_riemann(c["states"])
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(a, a.shape[1]), c["u"]), "initial state differs"
+    b = torch.empty_like(a)
+    sim = Simulation(s)
+    res, iters, rt = sim.run(a, b, c["cfl"], c["res"], c["sim_time"], c["max_iters"])
+    assert iters == c["steps"]
+    assert abs(rt - c["run_time"]) <= 1e-12 * c["run_time"]
+    # whole runs accumulate FMA rounding over every step: 1e-9 here; the
+    # per-step bar of 1e-12 is checked step by step below
+    assert rel_err(to_host(res, res.shape[1]), c["out"]) < 1e-9
+
+
+# ---- step-by-step parity with the oracle ----------------------------------
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_tube_per_step_parity(cuda, oracle, dtype, seed):
+    """1-D N=400 Riemann tube (HLLC, van Leer, CFL 0.9, to t = 0.25/max ws):
+    at every step the GPU step applied to the oracle's state matches the
+    oracle's next state."""
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    shape = (400,)
+    npdt = NPDT[dtype]
+    u = oracle.fill_riemann(shape, riemann_states(seed, 1), GAMMA, dtype=npdt)
+    s = SplitSolver(shape, dtype=dtype, gamma=GAMMA)
+    t_end = 0.25 / float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+    t = 0.0
+    steps = 0
+    worst = 0.0
+    a = torch.empty((3, 400), dtype=torch.float64 if dtype == "f64" else torch.float32,
+                    device="cuda")
+    b = torch.empty_like(a)
+    while t < t_end and steps < 2000:
+        ws = float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+        dt = npdt(0.9 * (1.0 / 400) / ws)
+        dtdh = npdt(float(dt) / (1.0 / 400))
+        nxt = oracle.sweep(shape, 0, u, npdt(GAMMA), dtdh)
+        a.copy_(torch.from_numpy(u))
+        s.sweep(a, b, 0, float(dtdh))
+        worst = max(worst, rel_err(b.cpu().numpy(), nxt))
+        u = nxt
+        t += float(dt)
+        steps += 1
+    assert steps > 50
+    assert worst < TOL[dtype], f"worst per-step error {worst:.3e} over {steps} steps"
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("flux", ["hllc", "force"])
+def test_quadrant_2d_per_step_parity(cuda, oracle, dtype, flux):
+    """2-D four-quadrant problem, 96 x 80 (partial tiles in both dims): each
+    step's x and y sweeps against the oracle, ten steps, CFL 0.8."""
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    shape = (96, 80)
+    npdt = NPDT[dtype]
+    u = oracle.fill_riemann(shape, riemann_states(11, 2), GAMMA, dtype=npdt)
+    s = SplitSolver(shape, dtype=dtype, flux=flux, gamma=GAMMA)
+    res = 1.0 / 96
+    worst = 0.0
+    for _ in range(10):
+        ws = float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+        dt = npdt(0.8 * res / ws)
+        dtdh = npdt(float(dt) / res)
+        mid = oracle.sweep(shape, 0, u, npdt(GAMMA), dtdh, flux=flux)
+        nxt = oracle.sweep(shape, 1, mid, npdt(GAMMA), dtdh, flux=flux)
+        a = to_dev(u, dtype)
+        b = torch.empty_like(a)
+        s.sweep(a, b, 0, float(dtdh))
+        worst = max(worst, rel_err(b.cpu().numpy(), mid))
+        a.copy_(torch.from_numpy(mid))
+        s.sweep(a, b, 1, float(dtdh))
+        worst = max(worst, rel_err(b.cpu().numpy(), nxt))
+        u = nxt
+    assert worst < TOL[dtype], f"worst per-step error {worst:.3e}"
+
+
+# ---- policy coverage on smooth data --------------------------------------
+
+POLICIES = [
+    ("hllc", "vanleer", "muscl", True), ("force", "vanleer", "muscl", True),
+    ("lf", "superbee", "muscl", True), ("richtmyer", "vanleer", "muscl", True),
+    ("hllc", "superbee", "basic", True), ("hllc", "vanleer", "muscl", False),
+]
+
+
+@pytest.mark.parametrize("shape", [(300,), (70, 45), (20, 13, 11)], ids=["1d", "2d", "3d"])
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("pol", POLICIES, ids=lambda p: "-".join(str(x) for x in p))
+def test_policy_sweeps(cuda, oracle, shape, dtype, pol):
+    flux, lim, recon, flatten = pol
+    npdt = NPDT[dtype]
+    D = len(shape)
+    u = oracle.prim_to_cons(random_prim(shape, 7 + D, smooth=True), GAMMA).astype(npdt)
+    ws = float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+    dtdh = npdt(0.5 / ws)
+    for dim in range(D):
+        for reflect in (0, (1 << D) - 1):
+            ref = oracle.sweep(shape, dim, u, npdt(GAMMA), dtdh, flux=flux, limiter=lim,
+                               recon=recon, flatten=flatten, reflect=reflect)
+            out = gpu_sweep(shape, dim, u, float(dtdh), dtype=dtype, flux=flux, limiter=lim,
+                            recon=recon, flatten=flatten, reflect=reflect)
+            assert rel_err(out, ref) < TOL[dtype], (dim, reflect)
+
+
+def test_flattening_active_parity(cuda, oracle):
+    """A strong shock front so that chi < 1 somewhere, in every dimension."""
+    shape = (64, 48)
+    prim = np.zeros((4, 64 * 48))
+    x = np.tile(np.arange(64), 48)
+    y = np.repeat(np.arange(48), 64)
+    prim[0] = np.where(x + y < 50, 5.0, 0.2)
+    prim[1] = np.where(x + y < 50, 800.0, 0.05)
+    prim[2] = np.where(x + y < 50, 1.5, -0.5)
+    prim[3] = np.where(x + y < 50, 1.0, -1.0)
+    u = oracle.prim_to_cons(prim, GAMMA)
+    ws = oracle.max_wavespeed(shape, u, GAMMA)
+    for dim in (0, 1):
+        ref = oracle.sweep(shape, dim, u, GAMMA, 0.8 / ws)
+        noflat = oracle.sweep(shape, dim, u, GAMMA, 0.8 / ws, flatten=False)
+        assert not np.array_equal(ref, noflat), "flattening never triggered"
+        out = gpu_sweep(shape, dim, u, 0.8 / ws)
+        assert rel_err(out, ref) < TOL["f64"]
+
+
+def test_pitch_padding(cuda, oracle):
+    """Component planes with a pitch larger than the cell count."""
+    shape = (50, 30)
+    u = oracle.prim_to_cons(random_prim(shape, 3, smooth=True), GAMMA)
+    ref = oracle.sweep(shape, 1, u, GAMMA, 0.001)
+    out = gpu_sweep(shape, 1, u, 0.001, pitch=1600)
+    assert rel_err(out, ref) < TOL["f64"]
+
+
+def test_fused_wavespeed_of_output(cuda, oracle):
+    shape = (128, 64)
+    u = oracle.prim_to_cons(random_prim(shape, 5, smooth=True), GAMMA)
+    out, ws = gpu_sweep(shape, 1, u, 0.002, want_ws=True)
+    ref = oracle.max_wavespeed(shape, out, GAMMA)
+    assert abs(ws - ref) <= 1e-14 * ref
+
+
+# ---- the device-resident loop ---------------------------------------------
+
+def test_loop_matches_host_loop(cuda, oracle):
+    """fl_sim_* (device-resident dt) against the oracle's time loop, 2-D."""
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    shape = (64, 64)
+    u = oracle.fill_riemann(shape, riemann_states(3, 2), GAMMA)
+    ref, steps, rt, dts = oracle.simulate(shape, u, GAMMA, 0.8, 1 / 64, 1e30, 15)
+    s = SplitSolver(shape, gamma=GAMMA)
+    a = to_dev(u, "f64")
+    b = torch.empty_like(a)
+    sim = Simulation(s)
+    sim.begin(a, b, 0.8, 1 / 64, 1e30, 15)
+    sim.steps(7)
+    it, t, done, _ = sim.status()
+    assert it == 7 and not done
+    sim.steps(8)
+    it, t, done, res = sim.status()
+    assert it == 15 and done
+    assert abs(t - rt) <= 1e-12 * rt
+    assert rel_err(res.cpu().numpy(), ref) < 1e-10
+
+
+@pytest.mark.parametrize("shape", [(257,), (65, 33), (17, 12, 10)])
+def test_reflective_box_conserves(cuda, shape):
+    """With reflective walls in every dimension no mass or energy leaves."""
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    D = len(shape)
+    s = SplitSolver(shape, gamma=GAMMA, boundary_mask=(1 << D) - 1)
+    st = riemann_states(40 + D, D)
+    st[:, 1] = np.clip(st[:, 1], 0.5, 50.0)       # moderate pressure ratios
+    a = s.fill_riemann(st)
+    m0 = a[0].sum().item()
+    e0 = a[1].sum().item()
+    b = torch.empty_like(a)
+    res, it, _ = Simulation(s).run(a, b, 0.6, 1.0 / shape[0], 1e30, 40)
+    assert it == 40
+    assert abs(res[0].sum().item() - m0) <= 1e-12 * m0
+    assert abs(res[1].sum().item() - e0) <= 1e-12 * e0
+
+
+def test_sim_time_stop_and_result_buffer(cuda, oracle):
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    shape = (400,)
+    u = oracle.fill_riemann(shape, riemann_states(0, 1), GAMMA)
+    t_end = 0.1 / oracle.max_wavespeed(shape, u, GAMMA)
+    ref, steps, rt, _ = oracle.simulate(shape, u, GAMMA, 0.9, 1 / 400, t_end, 10 ** 9)
+    s = SplitSolver(shape, gamma=GAMMA)
+    a = to_dev(u, "f64")
+    b = torch.empty_like(a)
+    res, it, t = Simulation(s).run(a, b, 0.9, 1 / 400, t_end, 10 ** 9)
+    assert it == steps
+    assert (res.data_ptr() == b.data_ptr()) == (steps % 2 == 1)
+    assert rel_err(res.cpu().numpy(), ref) < 1e-10
+
+
+def test_nan_state_reports_enan(cuda):
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.solver import Simulation, SplitSolver
+    s = SplitSolver((64,), gamma=GAMMA)
+    a = s.fill_riemann(np.array([[1.0, 1.0, 0.0], [0.125, 0.1, 0.0]]))
+    a[1, 10] = float("nan")
+    b = torch.empty_like(a)
+    with pytest.raises(capi.FlError) as e:
+        Simulation(s).run(a, b, 0.9, 1 / 64, 1.0, 100)
+    assert e.value.code == capi.FL_ENAN
+
+
+def test_split_solve_swaps_like_reference(cuda, oracle):
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    for shape in [(40,), (40, 24), (12, 10, 8)]:
+        u = oracle.prim_to_cons(random_prim(shape, 1, smooth=True), GAMMA)
+        s = SplitSolver(shape, gamma=GAMMA)
+        a = to_dev(u, "f64")
+        b = torch.empty_like(a)
+        i, o = s.solve(a, b, 0.001)
+        ref = u
+        for d in range(len(shape)):
+            ref = oracle.sweep(shape, d, ref, GAMMA, 0.001)
+        # the reference leaves the result in `out` after swapping iterators
+        assert o.data_ptr() == (a if len(shape) % 2 == 0 else b).data_ptr()
+        assert rel_err(o.cpu().numpy(), ref) < TOL["f64"]
+
+
+def test_fill_riemann_bit_exact(cuda, oracle):
+    from fluidity_b200.solver import SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    for shape in [(400,), (97, 50), (9, 8, 7)]:
+        D = len(shape)
+        st = riemann_states(5, D)
+        for dtype in ("f64", "f32"):
+            s = SplitSolver(shape, dtype=dtype, gamma=GAMMA)
+            got = s.fill_riemann(st).cpu().numpy()
+            ref = oracle.fill_riemann(shape, st, GAMMA, dtype=NPDT[dtype])
+            assert np.array_equal(got, ref)
+
+
+def test_aos_soa_round_trip(cuda):
+    import torch
+    from fluidity_b200 import capi
+    lib = capi.load()
+    g = capi.Grid.make((33, 17), pitch=600)
+    soa = torch.randn(4, 600, dtype=torch.float64, device="cuda")
+    aos = torch.empty(33 * 17 * 4, dtype=torch.float64, device="cuda")
+    back = torch.zeros_like(soa)
+    capi.check(lib.fl_soa_to_aos(C.byref(g), 0, C.c_void_p(soa.data_ptr()),
+                                 C.c_void_p(aos.data_ptr()), None))
+    capi.check(lib.fl_aos_to_soa(C.byref(g), 0, C.c_void_p(aos.data_ptr()),
+                                 C.c_void_p(back.data_ptr()), None))
+    torch.cuda.synchronize()
+    n = 33 * 17
+    assert torch.equal(aos.view(n, 4).t(), soa[:, :n])
+    assert torch.equal(back[:, :n], soa[:, :n])
+
+
+def test_repeatable_bitwise(cuda, oracle):
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    s = SplitSolver((200, 150), gamma=GAMMA, flux="force")
+    outs = []
+    for _ in range(2):
+        a = s.fill_riemann(riemann_states(9, 2))
+        b = torch.empty_like(a)
+        res, _, _ = Simulation(s).run(a, b, 0.8, 1 / 200, 1e30, 12)
+        outs.append(res.clone())
+    assert torch.equal(outs[0], outs[1])
