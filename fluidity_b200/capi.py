@@ -66,6 +66,11 @@ def policy_bits(dtype: str = "f64", flux: str = "hllc", limiter: str = "vanleer"
     return bits
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [("dims", C.c_int32), ("n", C.c_int64 * 2), ("offset", C.c_int64),
+                ("pitch", C.c_int64), ("res", C.c_double)]
+
+
 # name -> (restype, argtypes); every symbol of include/fluidity_b200.h
 _P = C.c_void_p
 _G = C.POINTER(Grid)
@@ -89,6 +94,25 @@ PROTOTYPES = {
                                 C.POINTER(C.c_int), C.POINTER(_P)]),
     "fl_simulate": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P,
                               C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(_P)]),
+    "fl_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(BatchDesc), C.c_int32, C.c_double,
+                                  C.c_uint32, C.c_uint32]),
+    "fl_batch_destroy": (C.c_int, [_P]),
+    "fl_batch_begin": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_int64, _P]),
+    "fl_batch_steps": (C.c_int, [_P, C.c_int64, _P]),
+    "fl_batch_capture": (C.c_int, [_P, C.c_int64]),
+    "fl_batch_launch": (C.c_int, [_P, _P]),
+    "fl_batch_status": (C.c_int, [_P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_int32)]),
+    "fl_batch_autotune": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
+    "fl_batch_tuning": (C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
+    "fl_adjoint_sweep": (C.c_int, [_G, C.c_int, _P, _P, _P, C.c_double, C.c_double, C.c_uint32,
+                                   C.c_uint32, _P]),
+    "fl_adj_create": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,
+                                C.c_int64, C.c_int64]),
+    "fl_adj_destroy": (C.c_int, [_P]),
+    "fl_adj_forward": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.POINTER(C.c_double), _P]),
+    "fl_adj_dtdh": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "fl_adj_backward": (C.c_int, [_P, _P, _P, _P]),
 }
 
 _lib = None

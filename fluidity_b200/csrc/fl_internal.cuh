@@ -55,4 +55,8 @@ enum : int {
   kENoMem = 5,
 };
 
+// Records the message returned by fl_last_error_string() (thread-local) and
+// returns code.  Defined in fl_api.cu.
+int set_error(int code, const char* fmt, ...);
+
 }  // namespace fl

@@ -10,23 +10,32 @@
 // (state/state.hpp:88-98).  NC = D + 2.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+
+// Functions are host + device so that the host tests of the adjoint can run
+// them on the CPU; kernels use them on the device.
+#if defined(__CUDACC__)
+#define FL_HD __host__ __device__ __forceinline__
+#else
+#define FL_HD inline
+#endif
 
 namespace fl {
 
 enum FluxKind : int { kHllc = 0, kForce = 1, kLaxFriedrichs = 2, kRichtmyer = 3 };
 enum LimiterKind : int { kVanLeer = 0, kSuperbee = 1 };
 
-template <typename T> __device__ __forceinline__ T fl_sqrt(T x);
-template <> __device__ __forceinline__ double fl_sqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float fl_sqrt<float>(float x) { return sqrtf(x); }
-template <typename T> __device__ __forceinline__ T fl_abs(T x);
-template <> __device__ __forceinline__ double fl_abs<double>(double x) { return fabs(x); }
-template <> __device__ __forceinline__ float fl_abs<float>(float x) { return fabsf(x); }
+template <typename T> FL_HD T fl_sqrt(T x);
+template <> FL_HD double fl_sqrt<double>(double x) { return std::sqrt(x); }
+template <> FL_HD float fl_sqrt<float>(float x) { return std::sqrt(x); }
+template <typename T> FL_HD T fl_abs(T x);
+template <> FL_HD double fl_abs<double>(double x) { return std::fabs(x); }
+template <> FL_HD float fl_abs<float>(float x) { return std::fabs(x); }
 
 // std::min / std::max as the reference's <algorithm> defines them.
-template <typename T> __device__ __forceinline__ T std_min(T a, T b) { return (b < a) ? b : a; }
-template <typename T> __device__ __forceinline__ T std_max(T a, T b) { return (a < b) ? b : a; }
+template <typename T> FL_HD T std_min(T a, T b) { return (b < a) ? b : a; }
+template <typename T> FL_HD T std_max(T a, T b) { return (a < b) ? b : a; }
 
 template <typename T, int D>
 struct Cons {
@@ -36,13 +45,13 @@ struct Cons {
 
 // velocity m_d / rho (state_impl.hpp:88-96)
 template <typename T, int D>
-__device__ __forceinline__ T velocity(const Cons<T, D>& u, int d) {
+FL_HD T velocity(const Cons<T, D>& u, int d) {
   return u.v[2 + d] / u.v[0];
 }
 
 // (gamma - 1) (E - 0.5 rho sum_d (m_d / rho)^2) (state_impl.hpp:117-128, 49-61)
 template <typename T, int D>
-__device__ __forceinline__ T pressure(const Cons<T, D>& u, T gamma) {
+FL_HD T pressure(const Cons<T, D>& u, T gamma) {
   T sum = T(0);
 #pragma unroll
   for (int d = 0; d < D; ++d) {
@@ -55,7 +64,7 @@ __device__ __forceinline__ T pressure(const Cons<T, D>& u, T gamma) {
 // Conservative physical flux in dimension d, given its velocity and pressure
 // (state_impl.hpp:293-310, make_other_fluxes 228-244).
 template <typename T, int D>
-__device__ __forceinline__ void flux_vp(const Cons<T, D>& u, int d, T v, T p,
+FL_HD void flux_vp(const Cons<T, D>& u, int d, T v, T p,
                                         Cons<T, D>& f) {
   f.v[0] = u.v[2 + d];
   f.v[2 + d] = u.v[2 + d] * v + p;
@@ -66,20 +75,20 @@ __device__ __forceinline__ void flux_vp(const Cons<T, D>& u, int d, T v, T p,
 }
 
 template <typename T, int D>
-__device__ __forceinline__ void flux(const Cons<T, D>& u, int d, T gamma,
+FL_HD void flux(const Cons<T, D>& u, int d, T gamma,
                                      Cons<T, D>& f) {
   flux_vp(u, d, velocity(u, d), pressure(u, gamma), f);
 }
 
 // sqrt(gamma p / rho) (material/ideal_gas.hpp:75-78)
 template <typename T, int D>
-__device__ __forceinline__ T sound_speed_p(const Cons<T, D>& u, T gamma, T p) {
+FL_HD T sound_speed_p(const Cons<T, D>& u, T gamma, T p) {
   return fl_sqrt<T>(gamma * p / u.v[0]);
 }
 
 // max_d |u_d| + a (state_impl.hpp:167-178)
 template <typename T, int D>
-__device__ __forceinline__ T max_wavespeed(const Cons<T, D>& u, T gamma) {
+FL_HD T max_wavespeed(const Cons<T, D>& u, T gamma) {
   T m = fl_abs<T>(velocity(u, 0));
 #pragma unroll
   for (int d = 1; d < D; ++d) m = std_max(m, fl_abs<T>(velocity(u, d)));
@@ -89,7 +98,7 @@ __device__ __forceinline__ T max_wavespeed(const Cons<T, D>& u, T gamma) {
 // ---- HLLC (flux_method/flux_hllc.hpp:56-245) ---------------------------
 
 template <typename T, int D>
-__device__ __forceinline__ void hllc_star(const Cons<T, D>& u, int d, T s, T sstar,
+FL_HD void hllc_star(const Cons<T, D>& u, int d, T s, T sstar,
                                           T vel, T p, Cons<T, D>& out) {
   const T sf = s - vel;
   const T scale = sf / (s - sstar);
@@ -100,7 +109,7 @@ __device__ __forceinline__ void hllc_star(const Cons<T, D>& u, int d, T s, T sst
 }
 
 template <typename T, int D>
-__device__ __forceinline__ void hllc(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
+FL_HD void hllc(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
                                      T gamma, Cons<T, D>& f) {
   const T pl = pressure(ul, gamma), pr = pressure(ur, gamma);
   const T vl = velocity(ul, d), vr = velocity(ur, d);
@@ -137,7 +146,7 @@ __device__ __forceinline__ void hllc(const Cons<T, D>& ul, const Cons<T, D>& ur,
 // ---- FORCE = (LF + Richtmyer) / 2 (flux_force.hpp:73-84) ----------------
 
 template <typename T, int D>
-__device__ __forceinline__ void lax_friedrichs_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
+FL_HD void lax_friedrichs_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
                                                   const Cons<T, D>& fl, const Cons<T, D>& fr,
                                                   T dtdh, Cons<T, D>& f) {
   // flux_lax_friedrichs.hpp:63-78; dhdt = 1 / dtdh
@@ -148,7 +157,7 @@ __device__ __forceinline__ void lax_friedrichs_ff(const Cons<T, D>& ul, const Co
 }
 
 template <typename T, int D>
-__device__ __forceinline__ void richtmyer_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
+FL_HD void richtmyer_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
                                              const Cons<T, D>& fl, const Cons<T, D>& fr,
                                              int d, T gamma, T dtdh, Cons<T, D>& f) {
   // flux_richtmyer.hpp:78-88
@@ -160,7 +169,7 @@ __device__ __forceinline__ void richtmyer_ff(const Cons<T, D>& ul, const Cons<T,
 }
 
 template <int FLUX, typename T, int D>
-__device__ __forceinline__ void riemann(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
+FL_HD void riemann(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
                                         T gamma, T dtdh, Cons<T, D>& f) {
   if constexpr (FLUX == kHllc) {
     hllc(ul, ur, d, gamma, f);
@@ -185,7 +194,7 @@ __device__ __forceinline__ void riemann(const Cons<T, D>& ul, const Cons<T, D>& 
 // ---- limiters (limiting/van_leer_limiter.hpp:65-74, superbee 72-89) -----
 
 template <typename T>
-__device__ __forceinline__ T limit_single(int limiter, T left, T right) {
+FL_HD T limit_single(int limiter, T left, T right) {
   const T r = left / right;
   if (limiter == kSuperbee) {
     if (r <= T(0) || right == T(0)) return T(0);
@@ -202,7 +211,7 @@ __device__ __forceinline__ T limit_single(int limiter, T left, T right) {
 // dimension) at c-1, c+1.  Ratio in T; sigma test and eta in double.
 
 template <typename T>
-__device__ __forceinline__ double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
+FL_HD double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
                                            T u_prev, T u_next) {
   const T u_factor = u_prev - u_next;
   const T dp = fl_abs<T>(p_next - p_prev);
@@ -211,6 +220,141 @@ __device__ __forceinline__ double chi_base(T p_next, T p_prev, T p_nnext, T p_pp
   const T z = dp / fl_abs<T>(p_nnext - p_pprev);
   const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
   return std_min(1.0, std_max(0.0, temp));
+}
+
+
+// ---- fast forms used by the sweep kernel ---------------------------------
+// One reciprocal per state replaces the reference's one division per
+// velocity (m_d / rho -> m_d * (1 / rho)); every other expression keeps the
+// reference's order.  The results differ from the reference by rounding only
+// (a few ulp), well inside the 1e-12 (FP64) / 1e-5 (FP32) per-step bars.
+
+template <typename T> FL_HD T fl_rcp(T x);
+#if defined(__CUDA_ARCH__)
+template <> FL_HD double fl_rcp<double>(double x) { return __drcp_rn(x); }
+template <> FL_HD float fl_rcp<float>(float x) { return __frcp_rn(x); }
+#else
+template <> FL_HD double fl_rcp<double>(double x) { return 1.0 / x; }
+template <> FL_HD float fl_rcp<float>(float x) { return 1.0f / x; }
+#endif
+
+// Primitive quantities derived from a conservative state.
+template <typename T, int D>
+struct Derived {
+  T rinv;   // 1 / rho
+  T v[D];   // velocities
+  T p;      // pressure
+};
+
+template <typename T, int D>
+FL_HD Derived<T, D> derive(const Cons<T, D>& u, T gm1) {
+  Derived<T, D> q;
+  q.rinv = fl_rcp<T>(u.v[0]);
+  T sum = T(0);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    q.v[d] = u.v[2 + d] * q.rinv;
+    sum += q.v[d] * q.v[d];
+  }
+  q.p = gm1 * (u.v[1] - T(0.5) * u.v[0] * sum);
+  return q;
+}
+
+template <typename T, int D>
+FL_HD void flux_q(const Cons<T, D>& u, const Derived<T, D>& q, int d,
+                                       Cons<T, D>& f) {
+  flux_vp(u, d, q.v[d], q.p, f);
+}
+
+// max_d |u_d| + sqrt(gamma p / rho)
+template <typename T, int D>
+FL_HD T max_wavespeed_q(const Derived<T, D>& q, T gamma) {
+  T m = fl_abs<T>(q.v[0]);
+#pragma unroll
+  for (int d = 1; d < D; ++d) m = std_max(m, fl_abs<T>(q.v[d]));
+  return m + fl_sqrt<T>(gamma * q.p * q.rinv);
+}
+
+// HLLC with precomputed side quantities; adi = (gamma + 1) / (2 gamma).
+template <typename T, int D>
+FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
+                                       const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
+                                       T gamma, T adi, Cons<T, D>& f) {
+  const T pl = ql.p, pr = qr.p, vl = ql.v[d], vr = qr.v[d];
+  const T al = fl_sqrt<T>(gamma * pl * ql.rinv);
+  const T ar = fl_sqrt<T>(gamma * pr * qr.rinv);
+  const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * (vr - vl) * (ur.v[0] + ul.v[0]) * (al + ar)));
+  const T p_star = std_max(T(0), p_pvrs);
+  const T wsl = (p_star <= pl) ? vl + (-al)
+                               : vl + (-al) * fl_sqrt<T>(T(1) + adi * (p_star / pl - T(1)));
+  if (T(0) <= wsl) { flux_vp(ul, d, vl, pl, f); return; }
+  const T wsr = (p_star <= pr) ? vr + ar
+                               : vr + ar * fl_sqrt<T>(T(1) + adi * (p_star / pr - T(1)));
+  if (T(0) >= wsr) { flux_vp(ur, d, vr, pr, f); return; }
+  const T factl = ul.v[0] * (wsl - vl);
+  const T factr = ur.v[0] * (wsr - vr);
+  const T sstar = (pr - pl + vl * factl - vr * factr) / (factl - factr);
+  // star state (flux_hllc.hpp:150-188) folded into F_K + S_K (U*_K - U_K)
+  const bool left = T(0) <= sstar;
+  const Cons<T, D>& u = left ? ul : ur;
+  const T s = left ? wsl : wsr;
+  const T vel = left ? vl : vr;
+  const T p = left ? pl : pr;
+  const T sf = s - vel;
+  const T scale = sf / (s - sstar);
+  flux_vp(u, d, vel, p, f);
+  Cons<T, D> st;
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c) st.v[c] = scale * u.v[c];
+  st.v[2 + d] = sstar * u.v[0] * scale;
+  st.v[1] = scale * (u.v[1] + u.v[0] * (sstar - vel) * (sstar + p / (u.v[0] * sf)));
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + s * (st.v[c] - u.v[c]);
+}
+
+template <int FLUX, typename T, int D>
+FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
+                                          const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
+                                          T gamma, T gm1, T adi, T dtdh, Cons<T, D>& f) {
+  if constexpr (FLUX == kHllc) {
+    hllc_q(ul, ql, ur, qr, d, gamma, adi, f);
+  } else {
+    Cons<T, D> fl, fr;
+    flux_q(ul, ql, d, fl);
+    flux_q(ur, qr, d, fr);
+    Cons<T, D> lf, ri;
+    if constexpr (FLUX != kRichtmyer) lax_friedrichs_ff(ul, ur, fl, fr, dtdh, lf);
+    if constexpr (FLUX != kLaxFriedrichs) {
+      Cons<T, D> m;
+#pragma unroll
+      for (int c = 0; c < D + 2; ++c)
+        m.v[c] = T(0.5) * (ul.v[c] + ur.v[c] + dtdh * (fl.v[c] - fr.v[c]));
+      flux_q(m, derive(m, gm1), d, ri);
+    }
+    if constexpr (FLUX == kLaxFriedrichs) {
+      f = lf;
+    } else if constexpr (FLUX == kRichtmyer) {
+      f = ri;
+    } else {
+#pragma unroll
+      for (int c = 0; c < D + 2; ++c) f.v[c] = T(0.5) * (lf.v[c] + ri.v[c]);
+    }
+  }
+}
+
+// The reference's van Leer slope 0.5 (bd + fd) * 2 min(r, 1) / (1 + r) with
+// r = bd / fd equals, in exact arithmetic, minmod(bd, fd): bd when
+// 0 < r <= 1, fd when r > 1, 0 when r <= 0 or fd == 0.  Superbee keeps the
+// reference's formula.
+template <typename T>
+FL_HD T limited_slope(int limiter, T bd, T fd) {
+  if (limiter == kSuperbee) {
+    T lim = T(0.5) * (bd + fd);
+    return lim * limit_single<T>(kSuperbee, bd, fd);
+  }
+  const bool same = (bd > T(0) && fd > T(0)) || (bd < T(0) && fd < T(0));
+  if (!same) return T(0);
+  return (fl_abs<T>(bd) <= fl_abs<T>(fd)) ? bd : fd;
 }
 
 }  // namespace fl

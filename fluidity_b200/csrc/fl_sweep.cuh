@@ -64,14 +64,21 @@ struct SweepGeom {
   static constexpr int F = F0 * F1 * F2;
   static constexpr int OUT = T0 * T1 * T2;
   static constexpr int THREADS = TS_::THREADS;
-  static constexpr size_t smem_bytes =
-      sizeof(T) * (size_t)(NC * R + R + 2 * NC * E + NC * F) + 64;
+  // shared memory: U (NC planes), P, velocities (D planes), chi bases (D
+  // planes) over the region; evolved faces ER, EL; face fluxes FX alias the
+  // velocity + chi planes (dead after stage C) when they fit.
+  static constexpr bool FX_ALIAS = 2 * D * R >= NC * F;
+  static constexpr size_t smem_elems =
+      (size_t)NC * R + R + 2 * D * R + 2 * NC * E + (FX_ALIAS ? 0 : NC * F);
+  static constexpr size_t smem_bytes = sizeof(T) * smem_elems + 64;
   __host__ __device__ static constexpr int rstride(int d) {
     return d == 0 ? 1 : (d == 1 ? R0 : R0 * R1);
   }
   __host__ __device__ static constexpr int estride(int d) {
     return d == 0 ? 1 : (d == 1 ? E0 : E0 * E1);
   }
+  __host__ __device__ static constexpr int tile(int d) { return d == 0 ? T0 : (d == 1 ? T1 : T2); }
+  __host__ __device__ static constexpr int halo(int d) { return d == 0 ? H0 : (d == 1 ? H1 : H2); }
 };
 
 __device__ __forceinline__ int64_t mirror_index(int64_t g, int64_t n, bool& flipped) {
@@ -156,13 +163,17 @@ sweep_kernel(SweepParams p) {
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
   const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
   const T gamma = (T)p.gamma;
+  const T gm1 = gamma - T(1);
+  const T adi = (gamma + T(1)) / (T(2) * gamma);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sU = reinterpret_cast<T*>(smem_raw);   // [NC][R]
   T* sP = sU + NC * G::R;                     // [R]
-  T* sER = sP + G::R;                         // [NC][E]
+  T* sV = sP + G::R;                          // [D][R] velocities
+  T* sChi = sV + D * G::R;                    // [D][R] chi bases
+  T* sER = sChi + D * G::R;                   // [NC][E]
   T* sEL = sER + NC * G::E;                   // [NC][E]
-  T* sFX = sEL + NC * G::E;                   // [NC][F]
+  T* sFX = G::FX_ALIAS ? sV : sEL + NC * G::E;  // [NC][F]
   __shared__ double s_red[NT / 32];
 
   const T* __restrict__ in = static_cast<const T*>(p.in);
@@ -172,8 +183,10 @@ sweep_kernel(SweepParams p) {
   const int64_t o0 = (int64_t)blockIdx.x * G::T0;
   const int64_t o1 = (int64_t)blockIdx.y * G::T1;
   const int64_t o2 = (int64_t)blockIdx.z * G::T2;
+  const bool muscl = !p.basic;
+  const bool flatten = muscl && p.flatten;
 
-  // ---- stage A: load tile + halo, mirror ghosts, pressure ---------------
+  // ---- stage A: load tile + halo, mirror ghosts, derived quantities -----
   for (int r = threadIdx.x; r < G::R; r += NT) {
     const int l0 = r % G::R0;
     const int l1 = (r / G::R0) % G::R1;
@@ -189,67 +202,89 @@ sweep_kernel(SweepParams p) {
     if (f0 && (p.reflect & 1u)) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
     if (D >= 2 && f1 && (p.reflect & 2u)) u.v[3] = (-(u.v[3] / u.v[0])) * u.v[0];
     if (D >= 3 && f2 && (p.reflect & 4u)) u.v[4] = (-(u.v[4] / u.v[0])) * u.v[0];
+    const Derived<T, D> q = derive(u, gm1);
 #pragma unroll
     for (int c = 0; c < NC; ++c) sU[c * G::R + r] = u.v[c];
-    sP[r] = pressure(u, gamma);
+    sP[r] = q.p;
+#pragma unroll
+    for (int d = 0; d < D; ++d) sV[d * G::R + r] = q.v[d];
   }
   __syncthreads();
 
-  // ---- stage C: flattening, limited slope, evolved face states ----------
+  // ---- stage B: flattening bases chi(c, d) for every cell and dimension
+  // that stage C reads (muscl_reconstructor.hpp:59-87) -------------------
+  if (flatten) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      // box, in tile coordinates: along S the evolve range [-1, T_S] widened
+      // by one more when d == S; along d != S the tile widened by one.
+      int lo[3], ext[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = 0;
+        ext[k] = (k < D) ? G::tile(k) : 1;
+      }
+      lo[S] = (d == S) ? -2 : -1;
+      ext[S] = G::tile(S) + ((d == S) ? 4 : 2);
+      if (d != S) { lo[d] = -1; ext[d] = G::tile(d) + 2; }
+      const int count = ext[0] * ext[1] * ext[2];
+      const int st = G::rstride(d);
+      const T* vd = sV + d * G::R;
+      for (int i = threadIdx.x; i < count; i += NT) {
+        const int c0 = i % ext[0] + lo[0];
+        const int c1 = (i / ext[0]) % ext[1] + lo[1];
+        const int c2 = i / (ext[0] * ext[1]) + lo[2];
+        const int q = ((c2 + G::H2) * G::R1 + (c1 + G::H1)) * G::R0 + (c0 + G::H0);
+        sChi[d * G::R + q] = (T)chi_base<T>(sP[q + st], sP[q - st], sP[q + 2 * st],
+                                            sP[q - 2 * st], vd[q - st], vd[q + st]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- stage C: limited slope, evolved face states -----------------------
   constexpr int SS = G::rstride(S);
   for (int e = threadIdx.x; e < G::E; e += NT) {
     const int e0 = e % G::E0;
     const int e1 = (e / G::E0) % G::E1;
     const int e2 = e / (G::E0 * G::E1);
-    // region coordinate: evolve coordinate is shifted by -1 along S
     const int q0 = e0 + G::H0 - (S == 0 ? 1 : 0);
     const int q1 = e1 + G::H1 - (S == 1 ? 1 : 0);
     const int q2 = e2 + G::H2 - (S == 2 ? 1 : 0);
     const int q = (q2 * G::R1 + q1) * G::R0 + q0;
-    Cons<T, D> u, um, up;
+    Cons<T, D> u;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      u.v[c] = sU[c * G::R + q];
-      um.v[c] = sU[c * G::R + q - SS];
-      up.v[c] = sU[c * G::R + q + SS];
-    }
+    for (int c = 0; c < NC; ++c) u.v[c] = sU[c * G::R + q];
     Cons<T, D> er, el;
-    if (p.basic) {
+    if (!muscl) {
       er = u;
       el = u;
     } else {
       T chi_v = T(1);
-      if (p.flatten) {
+      if (flatten) {
         chi_v = (sizeof(T) == 8) ? (T)DBL_MAX : (T)FLT_MAX;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
           const int st = G::rstride(d);
           const T diff = sP[q + st] - sP[q - st];
           const int sign = (T(0) < diff) - (diff < T(0));
-          const int qs = q + sign * st;
-          const T* vd = sU + (2 + d) * G::R;
-          const double c0 = chi_base<T>(sP[q + st], sP[q - st], sP[q + 2 * st], sP[q - 2 * st],
-                                        vd[q - st] / sU[q - st], vd[q + st] / sU[q + st]);
-          const double c1 = chi_base<T>(sP[qs + st], sP[qs - st], sP[qs + 2 * st], sP[qs - 2 * st],
-                                        vd[qs - st] / sU[qs - st], vd[qs + st] / sU[qs + st]);
-          chi_v = std_min(chi_v, (T)std_min(c0, c1));
+          const T* cd = sChi + d * G::R;
+          chi_v = std_min(chi_v, std_min(cd[q], cd[q + sign * st]));
         }
       }
       const T ch = chi_v * T(0.5);
       Cons<T, D> a, b;  // a = U - delta, b = U + delta
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const T bd = u.v[c] - um.v[c];
-        const T fd = up.v[c] - u.v[c];
-        T lim = T(0.5) * (bd + fd);
-        lim *= limit_single<T>(p.limiter, bd, fd);
-        const T delta = ch * lim;
+        const T um = sU[c * G::R + q - SS];
+        const T up = sU[c * G::R + q + SS];
+        const T delta = ch * limited_slope<T>(p.limiter, u.v[c] - um, up - u.v[c]);
         a.v[c] = u.v[c] - delta;
         b.v[c] = u.v[c] + delta;
       }
       Cons<T, D> fa, fb;
-      flux(a, S, gamma, fa);
-      flux(b, S, gamma, fb);
+      flux_q(a, derive(a, gm1), S, fa);
+      flux_q(b, derive(b, gm1), S, fb);
       const T hd = T(0.5) * dtdh;
       // right face: (U+d) + hd (F(U-d) - F(U+d)); left face: (U-d) + hd (F(U-d) - F(U+d))
 #pragma unroll
@@ -281,7 +316,7 @@ sweep_kernel(SweepParams p) {
       ul.v[c] = sER[c * G::E + el_idx];
       ur.v[c] = sEL[c * G::E + el_idx + ES];
     }
-    riemann<FLUX>(ul, ur, S, gamma, dtdh, fx);
+    riemann_q<FLUX>(ul, derive(ul, gm1), ur, derive(ur, gm1), S, gamma, gm1, adi, dtdh, fx);
 #pragma unroll
     for (int c = 0; c < NC; ++c) sFX[c * G::F + f] = fx.v[c];
   }
@@ -306,7 +341,7 @@ sweep_kernel(SweepParams p) {
       r.v[c] = sU[c * G::R + q] + dtdh * (sFX[c * G::F + fi] - sFX[c * G::F + fi + FS]);
 #pragma unroll
     for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-    if (want_ws) ws_max(ws_local, (double)max_wavespeed(r, gamma));
+    if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
   }
   if (want_ws)
     cta_wavespeed_commit<NT>(ws_local, p.ws_accum, p.ctrl, p.finalize, true, s_red);

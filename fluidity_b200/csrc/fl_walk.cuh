@@ -1,0 +1,256 @@
+// fl_walk.cuh -- register-streaming 2-D sweep kernel ("walker").
+//
+// Same arithmetic as sweep_kernel (fl_sweep.cuh): one dimensional sweep of
+// SplitSolver::invoke (solver/split_solver.hpp:138-162), MUSCL-Hancock with
+// flattening (reconstruction/muscl_reconstructor.hpp:59-172), one Riemann
+// solve per face, conservative update, optional fused max wavespeed.
+//
+// Mapping.  A warp owns 32 consecutive x columns and streams down a strip of
+// RY rows.  Every lane loads its column's state once per row (coalesced),
+// derives pressure and velocities once, and keeps sliding register windows
+// of the rows it still needs.  Neighbours along x come from warp shuffles;
+// neighbours along y come from the windows.  No shared-memory staging and no
+// block barriers.
+//   x sweep (S = 0): the stencil runs across lanes.  Lanes 0..31 hold columns
+//     x0-4 .. x0+27; flattening along x is valid on lanes 2..29, evolved faces
+//     on lanes 3..28, Riemann faces on lanes 4..28, updates on lanes 4..27
+//     (24 owned columns).  The y flattening bases come from the row windows.
+//   y sweep (S = 1): the stencil runs down the strip.  Lanes hold columns
+//     x0-3 .. x0+28; the x flattening needs lanes +-3, so lanes 3..28 (26)
+//     are owned.  Evolved faces, Riemann solves and updates follow the walk.
+// Rows and columns outside the domain are mirror ghosts, as in stage A of
+// sweep_kernel.
+#pragma once
+
+#include <cfloat>
+
+#include "fl_internal.cuh"
+#include "fl_numerics.cuh"
+#include "fl_sweep.cuh"
+
+namespace fl {
+
+template <typename T, int S>
+struct WalkCfg {
+  static constexpr int HX = (S == 0) ? 4 : 3;  // halo lanes on each side
+  static constexpr int OWN = 32 - 2 * HX;      // owned columns per warp
+  static constexpr int RY = 64;                // rows per warp strip
+  static constexpr int WARPS = 4;              // warps per CTA (stacked strips)
+  static constexpr int THREADS = 32 * WARPS;
+};
+
+template <typename T>
+__device__ __forceinline__ T shfl_up(T v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+template <typename T>
+__device__ __forceinline__ T shfl_dn(T v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+// One warp's strip: columns of column group bx, rows [y0, y0 + ry).  Stores
+// the updated rows and folds the wavespeed of each stored cell into
+// ws_local.  p.in / p.out / p.n / p.pitch describe the grid; dtdh is taken
+// from the caller.
+template <typename T, int S, int FLUX>
+__device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int64_t bx,
+                                              int64_t y0, int ry, double& ws_local,
+                                              bool want_ws) {
+  using W = WalkCfg<T, S>;
+  constexpr int D = 2;
+  constexpr int NC = 4;
+  const T gamma = (T)p.gamma;
+  const T gm1 = gamma - T(1);
+  const T adi = (gamma + T(1)) / (T(2) * gamma);
+  const T hd = T(0.5) * dtdh;
+  const bool muscl = !p.basic;
+  const bool flatten = muscl && p.flatten;
+  const T chi_init = (sizeof(T) == 8) ? (T)DBL_MAX : (T)FLT_MAX;
+
+  const T* __restrict__ in = static_cast<const T*>(p.in);
+  T* __restrict__ out = static_cast<T*>(p.out);
+  const int64_t pitch = p.pitch;
+  const int64_t n0 = p.n[0], n1 = p.n[1];
+  const int lane = threadIdx.x & 31;
+
+  const int64_t x = bx * W::OWN - W::HX + lane;
+  bool fx = false;
+  const int64_t gx = mirror_index(x, n0, fx);
+  const bool flip_x = fx && (p.reflect & 1u);
+  const bool flip_y_on = (p.reflect & 2u) != 0;
+  const bool owned = lane >= W::HX && lane < 32 - W::HX && x < n0;
+
+  if (y0 < n1) {
+    const int64_t y_end = (y0 + ry < n1) ? y0 + ry : n1;
+    // windows, index 4 = newest row k; row k - i at index 4 - i
+    Cons<T, D> U[5];
+    T P[5], VX[5], VY[5];
+    T CHY[3];  // chi_y of rows k-4, k-3, k-2
+    Cons<T, D> er_prev, f_prev;
+    const int64_t k_first = y0 - 3 - (S == 1 ? 1 : 0);
+    const int64_t k_last = y_end + (S == 1 ? 3 : 2);
+    for (int64_t k = k_first; k <= k_last; ++k) {
+      // ---- shift windows and load row k --------------------------------
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        U[i] = U[i + 1];
+        P[i] = P[i + 1];
+        VX[i] = VX[i + 1];
+        VY[i] = VY[i + 1];
+      }
+      {
+        bool fy = false;
+        const int64_t gy = mirror_index(k, n1, fy);
+        const int64_t gi = gy * n0 + gx;
+        Cons<T, D> u;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) u.v[c] = __ldg(in + c * pitch + gi);
+        if (flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
+        if (fy && flip_y_on) u.v[3] = (-(u.v[3] / u.v[0])) * u.v[0];
+        const Derived<T, D> q = derive(u, gm1);
+        U[4] = u;
+        P[4] = q.p;
+        VX[4] = q.v[0];
+        VY[4] = q.v[1];
+      }
+      // ---- y flattening base of row k - 2 (needs rows k-4..k) -----------
+      CHY[0] = CHY[1];
+      CHY[1] = CHY[2];
+      if (flatten) CHY[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VY[1], VY[3]);
+      const int64_t j = k - 3;  // evolve row
+      const bool evolve_row = (S == 0) ? (j >= y0) : (j >= y0 - 1);
+      if (!evolve_row) continue;
+
+      // ---- x flattening base of row j on this lane ----------------------
+      const T pj = P[1], vxj = VX[1];
+      const T p_r1 = shfl_dn(pj, 1), p_l1 = shfl_up(pj, 1);
+      const T p_r2 = shfl_dn(pj, 2), p_l2 = shfl_up(pj, 2);
+      T chx = T(1);
+      if (flatten) chx = (T)chi_base<T>(p_r1, p_l1, p_r2, p_l2, shfl_up(vxj, 1), shfl_dn(vxj, 1));
+      const T chx_r = shfl_dn(chx, 1), chx_l = shfl_up(chx, 1);
+
+      // ---- evolved face states of (lane, j) -------------------------------
+      const Cons<T, D>& u = U[1];
+      Cons<T, D> er, el;
+      if (!muscl) {
+        er = u;
+        el = u;
+      } else {
+        T chi_v = T(1);
+        if (flatten) {
+          const T dx = p_r1 - p_l1;
+          const int sx = (T(0) < dx) - (dx < T(0));
+          const T cx = std_min(chx, sx > 0 ? chx_r : (sx < 0 ? chx_l : chx));
+          const T dy = P[2] - P[0];
+          const int sy = (T(0) < dy) - (dy < T(0));
+          const T cy = std_min(CHY[1], sy > 0 ? CHY[2] : (sy < 0 ? CHY[0] : CHY[1]));
+          chi_v = std_min(std_min(chi_init, cx), cy);
+        }
+        const T ch = chi_v * T(0.5);
+        Cons<T, D> a, b;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          T um, up;
+          if (S == 0) {
+            um = shfl_up(u.v[c], 1);
+            up = shfl_dn(u.v[c], 1);
+          } else {
+            um = U[0].v[c];
+            up = U[2].v[c];
+          }
+          const T delta = ch * limited_slope<T>(p.limiter, u.v[c] - um, up - u.v[c]);
+          a.v[c] = u.v[c] - delta;
+          b.v[c] = u.v[c] + delta;
+        }
+        Cons<T, D> fa, fb;
+        flux_q(a, derive(a, gm1), S, fa);
+        flux_q(b, derive(b, gm1), S, fb);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const T df = fa.v[c] - fb.v[c];
+          er.v[c] = b.v[c] + hd * df;
+          el.v[c] = a.v[c] + hd * df;
+        }
+      }
+
+      if (S == 0) {
+        // face between lanes (lane-1, lane), then update of (lane, j)
+        Cons<T, D> ul, fx_l;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) ul.v[c] = shfl_up(er.v[c], 1);
+        riemann_q<FLUX>(ul, derive(ul, gm1), el, derive(el, gm1), 0, gamma, gm1, adi, dtdh, fx_l);
+        Cons<T, D> r;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const T fr = shfl_dn(fx_l.v[c], 1);
+          r.v[c] = u.v[c] + dtdh * (fx_l.v[c] - fr);
+        }
+        if (owned && j < y_end) {
+          const int64_t gi = j * n0 + x;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
+          if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+        }
+      } else {
+        if (j >= y0) {
+          // face (j-1, j) along y, then update of row j - 1
+          Cons<T, D> fxy;
+          riemann_q<FLUX>(er_prev, derive(er_prev, gm1), el, derive(el, gm1), 1, gamma, gm1,
+                          adi, dtdh, fxy);
+          if (j >= y0 + 1 && owned) {
+            const Cons<T, D>& uo = U[0];
+            Cons<T, D> r;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) r.v[c] = uo.v[c] + dtdh * (f_prev.v[c] - fxy.v[c]);
+            const int64_t gi = (j - 1) * n0 + x;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
+            if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+          }
+          f_prev = fxy;
+        }
+        er_prev = er;
+      }
+    }
+  }
+}
+
+// Warp max, then CTA max of the per-lane wavespeeds (all threads call).
+template <int WARPS>
+__device__ __forceinline__ double cta_max(double v, double* s_red) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) ws_max(v, __shfl_xor_sync(0xffffffffu, v, off));
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double m = s_red[0];
+#pragma unroll
+  for (int w = 1; w < WARPS; ++w) ws_max(m, s_red[w]);
+  return m;
+}
+
+template <typename T, int S, int FLUX>
+__global__ void __launch_bounds__(WalkCfg<T, S>::THREADS)
+walk_kernel_2d(SweepParams p) {
+  using W = WalkCfg<T, S>;
+  if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
+  const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
+  __shared__ double s_red[W::WARPS];
+  const int warp = threadIdx.x >> 5;
+  const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
+  double ws_local = 0.0;
+  const bool want_ws = (p.ws_accum != nullptr);
+  walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0, W::RY, ws_local, want_ws);
+  if (want_ws) {
+    const double m = cta_max<W::WARPS>(ws_local, s_red);
+    if (threadIdx.x == 0) {
+      atomicMax(p.ws_accum, (unsigned long long)__double_as_longlong(m));
+      if (p.finalize && p.ctrl) {
+        __threadfence();
+        const unsigned int total = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned int prev = atomicAdd(&p.ctrl->arrive, 1u);
+        if (prev == total - 1) {
+          __threadfence();
+          finalize_control(p.ctrl, true);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace fl

@@ -149,6 +149,96 @@ int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res,
                 double sim_time, int64_t max_iters, void* stream,
                 int64_t* iters, double* run_time, void** result);
 
+
+/* ---- batched solver: thousands of independent 1-D / 2-D problems ---------
+ * No reference counterpart (the reference solves one grid per simulator);
+ * each problem follows the time loop of SimulatorImpl::simulate with its own
+ * CFL time step.  Problem states live in caller-owned arenas: problem i's
+ * component c (order as above) of cell (x, y) is at
+ *     arena[offset_i + c * pitch_i + y * n_i[0] + x].
+ * Every result ends in arena_a; arena_b is the 2-D ping-pong partner (same
+ * size).  1-D problems run resident in shared memory (n <= 9000 in FP32,
+ * 4500 in FP64); 2-D problems run one batched launch per sweep.  HLLC or
+ * FORCE; policy and boundary mask apply to all problems. */
+typedef struct fl_batch_desc {
+  int32_t dims;       /* 1 or 2 */
+  int64_t n[2];       /* cells in x, y (n[1] ignored in 1-D) */
+  int64_t offset;     /* element offset of the problem's first plane */
+  int64_t pitch;      /* elements between the problem's component planes */
+  double res;         /* grid spacing dh */
+} fl_batch_desc;
+
+typedef struct fl_batch fl_batch;
+
+/* Uploads the problem list; allocates descriptors, per-problem time
+ * control and work lists on the current device. */
+int fl_batch_create(fl_batch** batch, const fl_batch_desc* problems, int32_t count,
+                    double gamma, uint32_t policy, uint32_t boundary_mask);
+int fl_batch_destroy(fl_batch* batch);
+
+/* Per-problem initial wavespeed and dt (cfl, stop time, step limit shared). */
+int fl_batch_begin(fl_batch* batch, void* arena_a, void* arena_b, double cfl,
+                   double sim_time, int64_t max_iters, void* stream);
+
+/* Enqueues nsteps time steps of every problem (1-D resident launches on a
+ * side stream, forked from and joined back into `stream`). */
+int fl_batch_steps(fl_batch* batch, int64_t nsteps, void* stream);
+
+/* Captures fl_batch_steps(nsteps) into a CUDA graph (after fl_batch_begin,
+ * for the arenas given there); fl_batch_launch replays it on `stream`. */
+int fl_batch_capture(fl_batch* batch, int64_t nsteps);
+int fl_batch_launch(fl_batch* batch, void* stream);
+
+/* Waits for `stream`; per-problem step counts and times (nullable arrays of
+ * `count` entries) and the number of finished problems.  FL_ENAN if a
+ * problem's wavespeed was not finite. */
+int fl_batch_status(fl_batch* batch, void* stream, int64_t* iters, double* run_time,
+                    int32_t* done_count);
+
+/* Autotuner: times the 1-D CTA width per size class and the 2-D warp-strip
+ * height per size class on copies of the arenas (trial_steps steps each)
+ * and keeps the fastest.  Allocates and frees its scratch copies. */
+int fl_batch_autotune(fl_batch* batch, void* arena_a, void* arena_b, int64_t trial_steps,
+                      void* stream);
+
+/* Current tuning: [1-D CTA widths of classes 0..2, 1-D class bounds (2),
+ * 2-D strip rows for small / mid / large sides]; n >= 8. */
+int fl_batch_tuning(const fl_batch* batch, int32_t* out, int32_t n);
+
+/* ---- discrete adjoint of the split step ------------------------------------
+ * No reference counterpart (the reference has no differentiation).  Reverse
+ * mode of the sweep with the HLLC wave region, shock/rarefaction choice,
+ * pressure clamp and limiter (minmod) selection frozen at the forward pass,
+ * the flattening coefficient chi frozen as a coefficient, and the CFL time
+ * step frozen.  1-D and 2-D grids, HLLC or FORCE, van Leer limiter. */
+
+/* lambda_in = (d sweep / d u_in)^T lambda_out for one dimensional sweep with
+ * the given dtdh (u_in: the sweep's input state). */
+int fl_adjoint_sweep(const fl_grid* grid, int dim, const void* u_in, const void* lambda_out,
+                     void* lambda_in, double gamma, double dtdh, uint32_t policy,
+                     uint32_t boundary_mask, void* stream);
+
+typedef struct fl_adj fl_adj;
+
+/* Allocates checkpoint storage for nsteps steps with a checkpoint every
+ * `interval` steps (<= 0: ceil(sqrt(nsteps))). */
+int fl_adj_create(fl_adj** adj, const fl_grid* grid, double gamma, uint32_t policy,
+                  uint32_t boundary_mask, int64_t nsteps, int64_t interval);
+int fl_adj_destroy(fl_adj* adj);
+
+/* Forward: nsteps steps from u0 into u_final (device), storing checkpoints.
+ * frozen_dtdh == NULL: CFL steps (cfl, res) computed on the device and
+ * recorded; else a host array of nsteps dt/dh values replayed as given. */
+int fl_adj_forward(fl_adj* adj, const void* u0, void* u_final, double cfl, double res,
+                   const double* frozen_dtdh, void* stream);
+
+/* The dt/dh of each step of the last forward pass (host array of nsteps). */
+int fl_adj_dtdh(const fl_adj* adj, double* out);
+
+/* Backward: lambda_0 = (d u_final / d u0)^T lambda_final, recomputing each
+ * checkpoint segment once. */
+int fl_adj_backward(fl_adj* adj, const void* lambda_final, void* lambda_0, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

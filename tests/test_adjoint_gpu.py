@@ -1,0 +1,118 @@
+"""The discrete adjoint on the GPU: single sweeps against finite differences
+of the forward sweep, the checkpointed time loop against central finite
+differences of the objective J = 0.5 ||p(T) - p_target||^2 along seeded
+directions (time steps frozen), and checkpoint-interval independence."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GAMMA = 1.4
+
+
+def _smooth_state(shape, seed):
+    from _util import random_prim
+    from oracle import oracle
+    return oracle.prim_to_cons(random_prim(shape, seed, smooth=True, mild=True), GAMMA)
+
+
+@pytest.mark.parametrize("shape,dim", [((64,), 0), ((40, 24), 0), ((40, 24), 1)])
+@pytest.mark.parametrize("flux", ["hllc", "force"])
+@pytest.mark.parametrize("reflect", [0, 1])
+def test_adjoint_sweep_transpose(cuda, shape, dim, flux, reflect):
+    """<lam, J du> (central differences of fl_split_sweep) = <J^T lam, du>."""
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.solver import SplitSolver
+    lib = capi.load()
+    u = torch.from_numpy(_smooth_state(shape, 3 + dim)).cuda()
+    s = SplitSolver(shape, flux=flux, gamma=GAMMA, boundary_mask=reflect)
+    ws = s.max_wavespeed(u).item()
+    dtdh = 0.6 / ws
+    g = torch.Generator(device="cpu").manual_seed(11)
+    lam = torch.randn(u.shape, generator=g, dtype=torch.float64).cuda()
+    du = (torch.randn(u.shape, generator=g, dtype=torch.float64) * 1e-2).cuda() * u.abs()
+    eps = 1e-6
+    up, um = torch.empty_like(u), torch.empty_like(u)
+    s.sweep(u + eps * du, up, dim, dtdh)
+    s.sweep(u - eps * du, um, dim, dtdh)
+    fd = torch.sum(lam * (up - um)).item() / (2 * eps)
+    lam_in = torch.empty_like(u)
+    capi.check(lib.fl_adjoint_sweep(C.byref(s.grid), dim, C.c_void_p(u.data_ptr()),
+                                    C.c_void_p(lam.data_ptr()), C.c_void_p(lam_in.data_ptr()),
+                                    GAMMA, dtdh, s.policy, reflect, None))
+    torch.cuda.synchronize()
+    ad = torch.sum(lam_in * du).item()
+    assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-12), (fd, ad)
+
+
+def _gradient_case(shape, nsteps, interval, seed=1):
+    import torch
+    from fluidity_b200.adjoint import (Adjoint, gaussian_density, objective, rollout,
+                                       state_from_density)
+    n = shape[0]
+    rho0 = gaussian_density(n, seed, count=8).requires_grad_(True)
+    adj = Adjoint(shape, nsteps, interval=interval)
+    target = gaussian_density(n, seed + 100, count=8)
+    with torch.no_grad():
+        pt = adj.forward(state_from_density(target), 0.7)
+        from fluidity_b200.adjoint import pressure
+        p_target = pressure(pt)
+    u0 = state_from_density(rho0)
+    uN = rollout(u0, adj, 0.7)
+    J = objective(uN, p_target)
+    J.backward()
+    return rho0, adj, p_target, J.item(), rho0.grad.clone()
+
+
+def test_adjoint_gradient_matches_finite_differences(cuda):
+    import torch
+    from fluidity_b200.adjoint import objective, random_directions, state_from_density
+    shape = (48, 48)
+    rho0, adj, p_target, J0, grad = _gradient_case(shape, nsteps=24, interval=5)
+    dts = adj.dtdh()
+    eps = 1e-6
+    worst = 0.0
+    for v in random_directions(rho0.numel(), 6, seed=7):
+        with torch.no_grad():
+            jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7, frozen_dtdh=dts),
+                           p_target).item()
+            jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7, frozen_dtdh=dts),
+                           p_target).item()
+        fd = (jp - jm) / (2 * eps)
+        ad = torch.dot(grad, v).item()
+        worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-30))
+    print(f"adjoint vs central differences: worst relative mismatch {worst:.3e}")
+    assert worst < 1e-6
+
+
+def test_adjoint_checkpoint_interval_independent(cuda):
+    import torch
+    _, _, _, J1, g1 = _gradient_case((32, 32), nsteps=13, interval=1)
+    _, _, _, J2, g2 = _gradient_case((32, 32), nsteps=13, interval=4)
+    _, _, _, J3, g3 = _gradient_case((32, 32), nsteps=13, interval=0)
+    assert J1 == J2 == J3
+    assert torch.equal(g1, g2) and torch.equal(g1, g3)
+
+
+def test_adjoint_1d(cuda):
+    """1-D tube: the rollout's gradient against central differences."""
+    import torch
+    from fluidity_b200.adjoint import Adjoint
+    shape = (128,)
+    u0 = torch.from_numpy(_smooth_state(shape, 21)).cuda()
+    adj = Adjoint(shape, 30, interval=6)
+    uN = adj.forward(u0, 0.8)
+    dts = adj.dtdh()
+    g = torch.Generator(device="cpu").manual_seed(5)
+    lamN = torch.randn(uN.shape, generator=g, dtype=torch.float64).cuda()
+    lam0 = adj.backward(lamN)
+    du = (torch.randn(u0.shape, generator=g, dtype=torch.float64) * 1e-2).cuda() * u0.abs()
+    eps = 1e-6
+    up = adj.forward(u0 + eps * du, 0.8, frozen_dtdh=dts)
+    um = adj.forward(u0 - eps * du, 0.8, frozen_dtdh=dts)
+    fd = torch.sum(lamN * (up - um)).item() / (2 * eps)
+    ad = torch.sum(lam0 * du).item()
+    assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
