@@ -94,6 +94,10 @@ PROTOTYPES = {
                                 C.POINTER(C.c_int), C.POINTER(_P)]),
     "fl_simulate": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P,
                               C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(_P)]),
+    "fl_simulate_noalloc": (C.c_int, [_G, C.c_double, C.c_uint32, C.c_uint32, _P, _P, C.c_double,
+                                      C.c_double, C.c_double, C.c_int64, _P,
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                      C.POINTER(_P)]),
     "fl_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(BatchDesc), C.c_int32, C.c_double,
                                   C.c_uint32, C.c_uint32]),
     "fl_batch_destroy": (C.c_int, [_P]),

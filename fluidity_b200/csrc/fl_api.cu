@@ -513,4 +513,65 @@ int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res, double si
   return kOk;
 }
 
+// ---- fl_simulate_noalloc: the time loop without any allocation ------------
+//
+// For callers that cannot call cudaMalloc -- code running where the CUDA
+// allocator is off limits (inside another framework's memory pool, a
+// real-time thread, a pre-allocated embedded deployment) -- the loop's only
+// scratch, its control block, lives in this file-scope device array instead
+// of the block fl_sim_create allocates.  Size: one StepControl (96 bytes),
+// whatever the grid: the loop never needs more.  Every GPU that loads the
+// library holds it until the process exits.  All calls on a device share
+// it and it keeps the last call's contents; fl_sim_begin's initialisation
+// kernel clears everything that must start at zero.  Calls that overlap on
+// the same GPU (two streams, two threads) race on it.
+static __device__ __align__(256) fl::StepControl g_noalloc_control[1];
+
+}  // extern "C"
+
+namespace {
+
+// Device address of g_noalloc_control, resolved once per device with that
+// device current.  (The host-side name of the array is a stand-in, not a
+// device address, and must never be handed to a kernel.)
+fl::StepControl* g_noalloc_addr[64] = {nullptr};
+
+}  // namespace
+
+extern "C" {
+
+int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
+                        uint32_t boundary_mask, void* a, void* b, double cfl, double res,
+                        double sim_time, int64_t max_iters, void* stream, int64_t* iters,
+                        double* run_time, void** result) {
+  static_assert(sizeof(g_noalloc_control) >= sizeof(fl::StepControl),
+                "the static scratch must hold one control block");
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if (!(gamma > 1.0)) return fail(kEInval, "gamma must exceed 1");
+  if (boundary_mask >> grid->dims) return fail(kEInval, "boundary_mask has bits beyond dims");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_simulate_noalloc");
+  if (dev < 0 || dev >= 64) return fail(kEInval, "device ordinal %d beyond the 64 supported", dev);
+  if (g_noalloc_addr[dev] == nullptr) {
+    // first call on this device: the set-up, outside any stream capture
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_control);
+    if (e != cudaSuccess) return cuda_fail(e, "fl_simulate_noalloc: cudaGetSymbolAddress");
+    g_noalloc_addr[dev] = static_cast<fl::StepControl*>(p);
+  }
+  fl_sim sim;
+  memset(&sim, 0, sizeof(sim));
+  sim.grid = *grid;
+  sim.pol = decode(policy);
+  sim.policy = policy;
+  sim.gamma = gamma;
+  sim.boundary = boundary_mask;
+  sim.device = dev;
+  sim.ctrl = g_noalloc_addr[dev];
+  return fl_simulate(&sim, a, b, cfl, res, sim_time, max_iters, stream, iters, run_time, result);
+}
+
 }  // extern "C"

@@ -149,6 +149,22 @@ int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res,
                 double sim_time, int64_t max_iters, void* stream,
                 int64_t* iters, double* run_time, void** result);
 
+/* fl_simulate without any allocation.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc (code that must not touch the CUDA
+ * allocator: inside another framework's memory pool, real-time threads,
+ * deployments that fix their memory up front).  Instead of the control block
+ * of fl_sim_create, the loop uses a fixed 96-byte block in a static device
+ * array of the library: one per GPU that loads it, held until the process
+ * exits; no grid size needs more.  Same arguments and result as
+ * fl_sim_create + fl_simulate.  The first call on a device resolves the
+ * array's device address, so make it before any stream capture.  Calls on
+ * the same GPU share the block: calls that overlap there (two streams or
+ * threads) race. */
+int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
+                        uint32_t boundary_mask, void* a, void* b, double cfl, double res,
+                        double sim_time, int64_t max_iters, void* stream, int64_t* iters,
+                        double* run_time, void** result);
+
 
 /* ---- batched solver: thousands of independent 1-D / 2-D problems ---------
  * No reference counterpart (the reference solves one grid per simulator);

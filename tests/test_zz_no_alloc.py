@@ -1,0 +1,82 @@
+"""fl_simulate_noalloc: the time loop for callers that cannot allocate.
+
+Some callers cannot call cudaMalloc -- code that must not touch the CUDA
+allocator, such as code inside another framework's memory pool, real-time
+threads, or deployments whose memory is fixed up front.  fl_simulate_noalloc
+runs the same loop as fl_sim_create + fl_simulate with its control block in
+a static device array of the library.  This test calls it through the C ABI
+twice in a row, the second call reusing the array left by the first, and
+checks both results against the allocating entry point.  The file name sorts
+last so that a run stopping at the first failure has run every other test.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from _util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+GAMMA = 1.4
+
+
+def _run_allocating(lib, capi, grid, policy, a, b, cfl, res, sim_time, steps):
+    h = C.c_void_p()
+    capi.check(lib.fl_sim_create(C.byref(h), C.byref(grid), GAMMA, policy, 0), lib)
+    it = C.c_int64()
+    rt = C.c_double()
+    out = C.c_void_p()
+    try:
+        capi.check(lib.fl_simulate(h, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), cfl,
+                                   res, sim_time, steps, None, C.byref(it), C.byref(rt),
+                                   C.byref(out)), lib)
+    finally:
+        lib.fl_sim_destroy(h)
+    return out.value, it.value, rt.value
+
+
+def _run_noalloc(lib, capi, grid, policy, a, b, cfl, res, sim_time, steps):
+    it = C.c_int64()
+    rt = C.c_double()
+    out = C.c_void_p()
+    capi.check(lib.fl_simulate_noalloc(C.byref(grid), GAMMA, policy, 0,
+                                       C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                       cfl, res, sim_time, steps, None, C.byref(it),
+                                       C.byref(rt), C.byref(out)), lib)
+    return out.value, it.value, rt.value
+
+
+@pytest.mark.parametrize("shape,states_seed", [((400,), 0), ((96, 80), 11)])
+def test_noalloc_matches_allocating_loop_twice(shape, states_seed):
+    import torch
+    from fluidity_b200 import build, capi
+    from fluidity_b200.solver import SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    assert torch.cuda.is_available()
+    build.build()
+    lib = capi.load()
+    s = SplitSolver(shape, gamma=GAMMA)
+    states = riemann_states(states_seed, len(shape))
+    res = 1.0 / shape[0]
+    # reference: the allocating entry point
+    ra, rb = s.fill_riemann(states), s.new_state()
+    ptr, ref_it, ref_rt = _run_allocating(lib, capi, s.grid, s.policy, ra, rb, 0.8, res, 1e30, 17)
+    ref = (ra if ptr == ra.data_ptr() else rb).cpu().numpy()
+    # two no-alloc calls in a row, the second with a different step count
+    # first, so that it starts from the contents the first one left
+    for steps in (17, 9):
+        a, b = s.fill_riemann(states), s.new_state()
+        ptr, it, rt = _run_noalloc(lib, capi, s.grid, s.policy, a, b, 0.8, res, 1e30, steps)
+        got = (a if ptr == a.data_ptr() else b).cpu().numpy()
+        if steps == 17:
+            assert it == ref_it == 17 and rt == ref_rt
+            assert rel_err(got, ref) < 1e-12
+        else:
+            ra2, rb2 = s.fill_riemann(states), s.new_state()
+            p2, it2, rt2 = _run_allocating(lib, capi, s.grid, s.policy, ra2, rb2, 0.8, res,
+                                           1e30, steps)
+            ref2 = (ra2 if p2 == ra2.data_ptr() else rb2).cpu().numpy()
+            assert it == it2 == 9 and rt == rt2
+            assert rel_err(got, ref2) < 1e-12
+    torch.cuda.synchronize()
