@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -49,6 +50,8 @@ def parse():
     p.add_argument("--flux", choices=["hllc", "force"], default="hllc")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -356,6 +359,10 @@ def run_ours(a, world, rank, local):
     }
     if variants:
         line["variants"] = variants
+    if rank == 0 and world == 1 and not a.no_batched:
+        line["batched"] = measure_batched()
+    if rank == 0 and world == 1 and not a.no_adjoint:
+        line["adjoint"] = measure_adjoint()
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(a)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores,
@@ -391,6 +398,135 @@ def measure_variant(a, dtype, flux, states, runs=3):
     cells = a.size * a.size
     return {"cell_updates_per_s": cells * T * runs / (total / 1e3),
             "sweep_gbs": 2 * 4 * elem * cells / sweep_s / 1e9, "steps_completed": it}
+
+
+def measure_batched(seed=3, steps=200, baseline_every=4):
+    """Batched workload: 3584 1-D problems (cells log-uniform in [64, 8192]) and
+    512 2-D problems (side log-uniform in [64, 512]), FP32 HLLC + van Leer, CFL
+    0.8, 200 steps each.  The batched solver (autotuned, time loop captured in
+    one CUDA graph) against per-problem launches of the plain step (fl_sim_*
+    per problem, all on one stream), the latter timed on every
+    `baseline_every`-th problem and reported as a rate."""
+    import torch
+    from fluidity_b200.batch import Batch, batched_workload
+    from fluidity_b200.solver import Simulation, SplitSolver
+    probs = batched_workload(seed=seed)
+    b = Batch(probs, dtype="f32", flux="hllc")
+    b.fill()
+    t0 = time.perf_counter()
+    tune = b.autotune(trial_steps=8)
+    tune_s = time.perf_counter() - t0
+    b.fill()
+    b.begin(0.8, 1e30, steps)
+    b.capture(steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    runs = []
+    for k in range(3):                     # first replay is the warm-up
+        b.fill()
+        torch.cuda.synchronize()
+        e0.record()
+        b.begin(0.8, 1e30, steps)
+        b.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        runs.append(e0.elapsed_time(e1))
+    it, _, done, rc = b.status(allow_nan=True)
+    ms = min(runs[1:])
+    cells = np.array([int(np.prod(s)) for s, _ in probs])
+    updates = float(np.sum(cells * it))
+    rate = updates / (ms / 1e3)
+    # per-problem launches of the plain step
+    sub = list(range(0, len(probs), baseline_every))
+    b.fill()
+    sims = []
+    for i in sub:
+        shape = probs[i][0]
+        s = SplitSolver(shape, dtype="f32", flux="hllc", pitch=b.pitches[i])
+        sims.append((s, Simulation(s), b.state(i, b.a), b.state(i, b.b)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s, sim, x, y in sims:
+        sim.begin(x, y, 0.8, 1.0 / s.shape[0], 1e30, steps)
+        sim.steps(steps)
+    torch.cuda.synchronize()
+    base_s = time.perf_counter() - t0
+    base_updates = 0.0
+    for (s, sim, x, y) in sims:
+        itb, _, _, _ = sim.status(allow_nan=True)
+        base_updates += float(np.prod(s.shape)) * itb
+    base_rate = base_updates / base_s
+    return {
+        "workload": "4096 problems: 3584 1-D (n log-uniform [64, 8192]) + 512 2-D "
+                    "(side log-uniform [64, 512]), FP32 HLLC + van Leer, CFL 0.8, 200 steps",
+        "cell_updates_per_s": rate, "ms_per_run": ms, "cell_updates": updates,
+        "problems_finished": int(done), "problems_stopped_nonfinite": int(np.sum(it < steps)),
+        "per_problem_launch_cell_updates_per_s": base_rate,
+        "per_problem_sample": f"every {baseline_every}th problem ({len(sub)} problems), "
+                              f"{base_s:.2f} s",
+        "speedup_vs_per_problem": rate / base_rate,
+        "autotune": tune, "autotune_s": tune_s, "graph": True,
+    }
+
+
+def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
+    """Gradient workload: 2-D n x n, density 1 + 32 seeded Gaussians, p = 1,
+    at rest; 300 HLLC/MUSCL steps at CFL 0.7; J = 0.5 ||p(T) - p_target||^2
+    with p_target from a second seed's field; dJ/d rho0 by the discrete
+    adjoint with ceil(sqrt(300)) = 18-step checkpoints, checked against
+    central differences along seeded unit directions (time steps frozen)."""
+    import torch
+    from fluidity_b200.adjoint import (Adjoint, gaussian_density, objective, pressure,
+                                       random_directions, rollout, state_from_density)
+    out = {}
+    for dtype in ("f64", "f32"):
+        tdt = torch.float64 if dtype == "f64" else torch.float32
+        adj = Adjoint((n, n), steps, dtype=dtype)
+        with torch.no_grad():
+            p_target = pressure(adj.forward(state_from_density(
+                gaussian_density(n, 2, dtype=tdt)), 0.7))
+        rho0 = gaussian_density(n, 1, dtype=tdt).requires_grad_(True)
+        u0 = state_from_density(rho0)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        uN = rollout(u0, adj, 0.7)            # warm-up (kernel set-up)
+        objective(uN, p_target).backward()
+        rho0.grad = None
+        torch.cuda.synchronize()
+        e[0].record()
+        uN = rollout(u0, adj, 0.7)
+        J = objective(uN, p_target)
+        e[1].record()
+        J.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+        grad = rho0.grad.detach().clone()
+        res = {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
+               "cost_ratio_backward_over_forward": bwd_ms / fwd_ms}
+        if dtype == "f64":
+            dts = adj.dtdh()
+            worst = 0.0
+            with torch.no_grad():
+                for v in random_directions(n * n, directions, seed=7):
+                    jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7,
+                                               frozen_dtdh=dts), p_target).item()
+                    jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7,
+                                               frozen_dtdh=dts), p_target).item()
+                    fd = (jp - jm) / (2 * eps)
+                    ad = torch.dot(grad, v).item()
+                    worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-300))
+            res.update({"fd_directions": directions, "fd_eps": eps,
+                        "fd_max_rel_err": worst})
+            out["grad_f64"] = grad
+        else:
+            g64 = out.pop("grad_f64")
+            res["rel_diff_vs_f64_gradient"] = (torch.norm(grad.double() - g64) /
+                                               torch.norm(g64)).item()
+        out[dtype] = res
+    out.pop("grad_f64", None)
+    out["workload"] = (f"2-D {n}x{n}, rho0 = 1 + 32 Gaussians, p = 1, at rest, {steps} HLLC "
+                       f"steps at CFL 0.7, checkpoint every {math.ceil(math.sqrt(steps))} steps")
+    return out
 
 
 def main():

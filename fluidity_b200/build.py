@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         return lib
     os.makedirs(BUILD, exist_ok=True)
     flags = NVCC_FLAGS + (extra_flags or [])
-    tag = "strict" if extra_flags else "default"
+    tag = os.path.splitext(os.path.basename(lib))[0]
 
     def compile_one(src: str) -> str:
         obj = os.path.join(BUILD, f"{tag}_" + os.path.basename(src) + ".o")

@@ -122,10 +122,13 @@ PROTOTYPES = {
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load the library (built by fluidity_b200.build); raise if absent."""
+def load(path: str | None = None):
+    """Load the library (built by fluidity_b200.build); raise if absent.
+    FLUIDITY_B200_LIB names an alternative build of the same library."""
     global _lib
-    if _lib is not None and path == LIB_PATH:
+    if path is None:
+        path = os.environ.get("FLUIDITY_B200_LIB", LIB_PATH)
+    if _lib is not None and path == os.environ.get("FLUIDITY_B200_LIB", LIB_PATH):
         return _lib
     if not os.path.exists(path):
         raise ImportError(
@@ -136,7 +139,7 @@ def load(path: str = LIB_PATH):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if path == LIB_PATH:
+    if path == os.environ.get("FLUIDITY_B200_LIB", LIB_PATH):
         _lib = lib
     return lib
 

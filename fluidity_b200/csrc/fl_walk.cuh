@@ -28,6 +28,19 @@
 #include "fl_numerics.cuh"
 #include "fl_sweep.cuh"
 
+#ifndef FL_WALK_CTAS_F64_X
+#define FL_WALK_CTAS_F64_X 4
+#endif
+#ifndef FL_WALK_CTAS_F64_Y
+#define FL_WALK_CTAS_F64_Y 3
+#endif
+#ifndef FL_WALK_CTAS_F32_X
+#define FL_WALK_CTAS_F32_X 6
+#endif
+#ifndef FL_WALK_CTAS_F32_Y
+#define FL_WALK_CTAS_F32_Y 5
+#endif
+
 namespace fl {
 
 template <typename T, int S>
@@ -37,6 +50,11 @@ struct WalkCfg {
   static constexpr int RY = 64;                // rows per warp strip
   static constexpr int WARPS = 4;              // warps per CTA (stacked strips)
   static constexpr int THREADS = 32 * WARPS;
+  // resident CTAs per SM the register allocation is held to: 65536 /
+  // (128 threads * MIN_CTAS) registers per thread.  Measured choice; the
+  // FL_WALK_CTAS_* macros override it for tuning builds.
+  static constexpr int MIN_CTAS = sizeof(T) == 8 ? (S == 0 ? FL_WALK_CTAS_F64_X : FL_WALK_CTAS_F64_Y)
+                                                 : (S == 0 ? FL_WALK_CTAS_F32_X : FL_WALK_CTAS_F32_Y);
 };
 
 template <typename T>
@@ -85,8 +103,17 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
     Cons<T, D> er_prev, f_prev;
     const int64_t k_first = y0 - 3 - (S == 1 ? 1 : 0);
     const int64_t k_last = y_end + (S == 1 ? 3 : 2);
+    // row k + 1 is loaded while row k is processed (global-load latency
+    // overlaps the arithmetic)
+    Cons<T, D> pre;
+    bool pre_fy = false;
+    {
+      const int64_t gy = mirror_index(k_first, n1, pre_fy);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
+    }
     for (int64_t k = k_first; k <= k_last; ++k) {
-      // ---- shift windows and load row k --------------------------------
+      // ---- shift windows and take row k ----------------------------------
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         U[i] = U[i + 1];
@@ -95,12 +122,13 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
         VY[i] = VY[i + 1];
       }
       {
-        bool fy = false;
-        const int64_t gy = mirror_index(k, n1, fy);
-        const int64_t gi = gy * n0 + gx;
-        Cons<T, D> u;
+        Cons<T, D> u = pre;
+        const bool fy = pre_fy;
+        if (k < k_last) {
+          const int64_t gy = mirror_index(k + 1, n1, pre_fy);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) u.v[c] = __ldg(in + c * pitch + gi);
+          for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
+        }
         if (flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
         if (fy && flip_y_on) u.v[3] = (-(u.v[3] / u.v[0])) * u.v[0];
         const Derived<T, D> q = derive(u, gm1);
@@ -225,7 +253,7 @@ __device__ __forceinline__ double cta_max(double v, double* s_red) {
 }
 
 template <typename T, int S, int FLUX>
-__global__ void __launch_bounds__(WalkCfg<T, S>::THREADS)
+__global__ void __launch_bounds__(WalkCfg<T, S>::THREADS, WalkCfg<T, S>::MIN_CTAS)
 walk_kernel_2d(SweepParams p) {
   using W = WalkCfg<T, S>;
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;

@@ -130,13 +130,17 @@ class Simulation:
     def steps(self, n, stream=None):
         capi.check(self.lib.fl_sim_steps(self.handle, int(n), _stream_ptr(stream)), self.lib)
 
-    def status(self, stream=None):
+    def status(self, stream=None, allow_nan=False):
+        """(iters, run_time, done, result buffer); a non-finite wavespeed raises
+        FlError(FL_ENAN) unless allow_nan, which reports the steps completed."""
         it = C.c_int64()
         rt = C.c_double()
         done = C.c_int()
         res = C.c_void_p()
-        capi.check(self.lib.fl_sim_status(self.handle, _stream_ptr(stream), C.byref(it),
-                                          C.byref(rt), C.byref(done), C.byref(res)), self.lib)
+        rc = self.lib.fl_sim_status(self.handle, _stream_ptr(stream), C.byref(it), C.byref(rt),
+                                    C.byref(done), C.byref(res))
+        if not (allow_nan and rc == capi.FL_ENAN):
+            capi.check(rc, self.lib)
         return int(it.value), float(rt.value), bool(done.value), self._bufs[res.value]
 
     def run(self, a, b, cfl, res, sim_time, max_iters, stream=None):

@@ -12,23 +12,31 @@ pytestmark = pytest.mark.gpu
 GAMMA = 1.4
 
 
-def _smooth_state(shape, seed):
+def _smooth_state(shape, seed, narrow_p=False):
     from _util import random_prim
     from oracle import oracle
-    return oracle.prim_to_cons(random_prim(shape, seed, smooth=True, mild=True), GAMMA)
+    prim = random_prim(shape, seed, smooth=True, mild=True)
+    if narrow_p:
+        # pressure within 1 +- 5 %: the flattening test |dp| / p > 0.33 never
+        # passes, so chi = 1 and freezing it is exact
+        prim[1] = 1.0 + 0.1 * (prim[1] - prim[1].min()) / (np.ptp(prim[1]) + 1e-30) - 0.05
+    return oracle.prim_to_cons(prim, GAMMA)
 
 
 @pytest.mark.parametrize("shape,dim", [((64,), 0), ((40, 24), 0), ((40, 24), 1)])
 @pytest.mark.parametrize("flux", ["hllc", "force"])
 @pytest.mark.parametrize("reflect", [0, 1])
-def test_adjoint_sweep_transpose(cuda, shape, dim, flux, reflect):
-    """<lam, J du> (central differences of fl_split_sweep) = <J^T lam, du>."""
+@pytest.mark.parametrize("flatten", [False, True])
+def test_adjoint_sweep_transpose(cuda, shape, dim, flux, reflect, flatten):
+    """<lam, J du> (central differences of fl_split_sweep) = <J^T lam, du>.
+    The adjoint freezes the flattening coefficient chi, so the check runs
+    without flattening, and with flattening on data where it stays inactive."""
     import torch
     from fluidity_b200 import capi
     from fluidity_b200.solver import SplitSolver
     lib = capi.load()
-    u = torch.from_numpy(_smooth_state(shape, 3 + dim)).cuda()
-    s = SplitSolver(shape, flux=flux, gamma=GAMMA, boundary_mask=reflect)
+    u = torch.from_numpy(_smooth_state(shape, 3 + dim, narrow_p=flatten)).cuda()
+    s = SplitSolver(shape, flux=flux, gamma=GAMMA, boundary_mask=reflect, flatten=flatten)
     ws = s.max_wavespeed(u).item()
     dtdh = 0.6 / ws
     g = torch.Generator(device="cpu").manual_seed(11)
