@@ -22,6 +22,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
               "-Xptxas", "-O3"]
+# The level-set and ghost-fluid kernels keep every product separately rounded
+# (no FMA contraction), so that they round exactly like the C restatement of
+# the reference's arithmetic; the split-solver kernels contract freely.
+FILE_FLAGS = {"fl_levelset.cu": ["--fmad=false"], "fl_mm.cu": ["--fmad=false"]}
 
 
 def nvcc() -> str:
@@ -54,7 +58,8 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
 
     def compile_one(src: str) -> str:
         obj = os.path.join(BUILD, f"{tag}_" + os.path.basename(src) + ".o")
-        cmd = [nvcc(), *ARCH, *flags, "-c", src, "-o", obj]
+        cmd = [nvcc(), *ARCH, *flags, *FILE_FLAGS.get(os.path.basename(src), []), "-c", src,
+               "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

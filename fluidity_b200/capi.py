@@ -117,6 +117,25 @@ PROTOTYPES = {
     "fl_adj_forward": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.POINTER(C.c_double), _P]),
     "fl_adj_dtdh": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "fl_adj_backward": (C.c_int, [_P, _P, _P, _P]),
+    "fl_ls_workspace_bytes": (C.c_int64, [_G]),
+    "fl_ls_velocity": (C.c_int, [_G, C.c_int, C.POINTER(_P), C.POINTER(_P), C.c_int64,
+                                 C.c_uint32, C.c_double, _P, _P]),
+    "fl_ls_advect": (C.c_int, [_G, _P, _P, C.c_double, C.c_double, _P, _P, _P]),
+    "fl_ls_project": (C.c_int, [C.c_int64, _P, _P, _P]),
+    "fl_ls_reinit": (C.c_int, [_G, _P, C.c_double, _P, _P, C.c_int, C.POINTER(C.c_int), _P]),
+    "fl_mm_create": (C.c_int, [C.POINTER(_P), _G, C.POINTER(C.c_double), C.c_uint32,
+                               C.c_double]),
+    "fl_mm_destroy": (C.c_int, [_P]),
+    "fl_mm_ghost": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _P]),
+    "fl_mm_stats": (C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
+    "fl_mm_set_states": (C.c_int, [_G, C.c_uint32, _P, _P, C.POINTER(C.c_double), C.c_double,
+                                   _P]),
+    "fl_mm_combine": (C.c_int, [_G, C.c_uint32, _P, _P, _P, _P]),
+    "fl_mm_begin": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                              C.c_int64, C.c_int]),
+    "fl_mm_steps": (C.c_int, [_P, C.c_int64, _P]),
+    "fl_mm_status": (C.c_int, [_P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                               C.POINTER(C.c_int), C.POINTER(_P), C.POINTER(_P)]),
 }
 
 _lib = None

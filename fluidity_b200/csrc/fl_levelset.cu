@@ -1,0 +1,395 @@
+// fl_levelset.cu -- level-set kernels of the multimaterial path and their C
+// ABI (include/fluidity_b200.h, fl_ls_*).
+//
+//  * fl_ls_velocity : interface-normal velocity from the first material
+//    containing each cell (levelset/cuda/velocity_initialization.cuh:108-143);
+//  * fl_ls_advect   : one TVD-RK3 step of phi_t + v |grad phi| = 0 with
+//    WENO-HJ5 one-sided derivatives and the Godunov upwind Hamiltonian
+//    (scheme/stencils/weno_hj_5.hpp, schemes/godunov_upwind.hpp,
+//    evaluators/levelset_hamiltonian.hpp, updaters/runge_kutta_3.hpp); every
+//    stage is one launch over the whole grid, so tile halos always hold the
+//    current stage (the reference's single-launch RK3 keeps stale halos
+//    between stages, scheme/cuda/evolve.cuh:51-157);
+//  * fl_ls_project  : two level sets without overlap or void
+//    (levelset/cuda/levelset_projection.cuh:54-67);
+//  * fl_ls_reinit   : signed-distance reinitialisation: sources next to the
+//    interface keep |phi| (scheme/cuda/fast_iterative_method.cuh:48-89, which
+//    seeds the signed value), every other cell
+//    relaxes to the fixed point of the Godunov local eikonal solve
+//    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles iterate in shared
+//    memory and only tiles next to a change run the next pass (active-tile
+//    list); the result takes the input's sign (set_signs, :96-112).
+// FP64 level sets on 2-D grids; out-of-domain reads mirror the domain.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "../../include/fluidity_b200.h"
+#include "fl_internal.cuh"
+
+namespace fl {
+namespace {
+
+__device__ __forceinline__ int64_t lmir(int64_t i, int64_t n) {
+  if (i < 0) i = -1 - i;
+  else if (i >= n) i = 2 * n - 1 - i;
+  return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+
+__device__ __forceinline__ double dmax_(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
+
+// WENO-HJ5 combination (weno_hj_5.hpp:85-144)
+__device__ __forceinline__ double weno_diff(double d1, double d2, double d3, double d4,
+                                            double d5) {
+  const double phi_1 = 2.0 * d1 - 7.0 * d2 + 11.0 * d3;
+  const double phi_2 = -d2 + 5.0 * d3 + 2.0 * d4;
+  const double phi_3 = 2.0 * d3 + 5.0 * d4 - d5;
+  const double f1 = 13.0 / 12.0, f2 = 1.0 / 4.0;
+  const double t1 = d1 - 2.0 * d2 + d3, t2 = d1 - 4.0 * d2 + 3.0 * d3;
+  const double t3 = d2 - 2 * d3 + d4, t4 = d2 - d4;
+  const double t5 = d3 - 2.0 * d4 + d5, t6 = 3.0 * d3 - 4.0 * d4 + d5;
+  double a1 = f1 * (t1 * t1) + f2 * (t2 * t2);
+  double a2 = f1 * (t3 * t3) + f2 * (t4 * t4);
+  double a3 = f1 * (t5 * t5) + f2 * (t6 * t6);
+  const double e =
+      10.0e-6 * dmax_(dmax_(dmax_(dmax_(d1 * d1, d2 * d2), d3 * d3), d4 * d4), d5 * d5) + 10.0e-99;
+  const double s1 = a1 + e, s2 = a2 + e, s3 = a3 + e;
+  a1 = 0.1 / (s1 * s1);
+  a2 = 0.6 / (s2 * s2);
+  a3 = 0.3 / (s3 * s3);
+  const double w_denom = (a1 + a2 + a3) * 6.0;
+  return (a1 * phi_1 + a2 * phi_2 + a3 * phi_3) / w_denom;
+}
+
+constexpr int LX = 32, LY = 8, LH = 3;
+constexpr int SX = LX + 2 * LH, SY = LY + 2 * LH;
+
+// One RK3 stage on a 32 x 8 tile staged with a 3-cell halo.
+//   stage 1: out = phi_n - dt H(phi_n)
+//   stage 2: out = 0.75 phi_n + 0.25 (s - dt H(s))
+//   stage 3: out = (1/3) phi_n + (2/3) (s - dt H(s))
+template <int STAGE>
+__global__ void __launch_bounds__(LX * LY) ls_rk3_kernel(const double* __restrict__ phi_n,
+                                                         const double* __restrict__ s,
+                                                         const double* __restrict__ vel,
+                                                         double dt, double h, int64_t nx,
+                                                         int64_t ny, double* __restrict__ out) {
+  __shared__ double tile[SY][SX + 1];
+  const int64_t x0 = (int64_t)blockIdx.x * LX, y0 = (int64_t)blockIdx.y * LY;
+  const double* src = (STAGE == 1) ? phi_n : s;
+  for (int i = threadIdx.x; i < SX * SY; i += LX * LY) {
+    const int lx = i % SX, ly = i / SX;
+    tile[ly][lx] = src[lmir(y0 - LH + ly, ny) * nx + lmir(x0 - LH + lx, nx)];
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % LX, ty = threadIdx.x / LX;
+  const int64_t x = x0 + tx, y = y0 + ty;
+  if (x >= nx || y >= ny) return;
+  const int cx = tx + LH, cy = ty + LH;
+  const int64_t i = y * nx + x;
+  const double v = vel[i];
+  const double h1 = 1.0 / h;
+  double r = 0.0;
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    double p[7];
+#pragma unroll
+    for (int k = -3; k <= 3; ++k) p[k + 3] = (d == 0) ? tile[cy][cx + k] : tile[cy + k][cx];
+    const double bk = weno_diff(h1 * (p[1] - p[0]), h1 * (p[2] - p[1]), h1 * (p[3] - p[2]),
+                                h1 * (p[4] - p[3]), h1 * (p[5] - p[4]));
+    const double fw = weno_diff(h1 * (p[6] - p[5]), h1 * (p[5] - p[4]), h1 * (p[4] - p[3]),
+                                h1 * (p[3] - p[2]), h1 * (p[2] - p[1]));
+    double b, w;
+    if (v <= 0.0) {
+      b = dmax_(bk, 0.0);
+      w = dmin_(fw, 0.0);
+    } else {
+      b = dmin_(bk, 0.0);
+      w = dmax_(fw, 0.0);
+    }
+    r += dmax_(b * b, w * w);
+  }
+  const double H = v * sqrt(r);
+  const double cur = tile[cy][cx];
+  if (STAGE == 1) {
+    out[i] = cur - dt * H;
+  } else if (STAGE == 2) {
+    out[i] = 0.75 * phi_n[i] + 0.25 * (cur - dt * H);
+  } else {
+    const double f13 = 1.0 / 3.0, f23 = 2.0 * f13;
+    out[i] = (f13 * phi_n[i]) + (f23 * (cur - dt * H));
+  }
+}
+
+template <typename T>
+__global__ void ls_velocity_kernel(int64_t nx, int64_t ny, int nmat, const double* phi0,
+                                   const double* phi1, const T* u0, const T* u1, int64_t pitch,
+                                   double h, double* vel) {
+  const int64_t n = nx * ny;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = i % nx, y = i / nx;
+    double v = 0.0;
+    for (int m = 0; m < nmat; ++m) {
+      const double* f = m == 0 ? phi0 : phi1;
+      const T* u = m == 0 ? u0 : u1;
+      if (!(f[i] <= 0.0 || f[i] <= -0.0)) continue;
+      const double fact = 0.5 / h;
+      const double g0 = fact * (f[y * nx + lmir(x + 1, nx)] - f[y * nx + lmir(x - 1, nx)]);
+      const double g1 = fact * (f[lmir(y + 1, ny) * nx + x] - f[lmir(y - 1, ny) * nx + x]);
+      const double s = sqrt(g0 * g0 + g1 * g1);
+      const double rho = (double)u[i];
+      v = ((double)u[2 * pitch + i] / rho) * (g0 / s) + ((double)u[3 * pitch + i] / rho) * (g1 / s);
+      break;
+    }
+    vel[i] = v;
+  }
+}
+
+__global__ void ls_project_kernel(int64_t n, double* a, double* b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double avg = __dmul_rn(0.5, a[i] + b[i]);  // no contraction into the subtraction
+    a[i] -= avg;
+    b[i] = -a[i];
+  }
+}
+
+// ---- reinitialisation ------------------------------------------------------
+
+constexpr int FT = 16;                 // tile side
+constexpr int FIM_INNER = 24;          // in-tile relaxation rounds per pass
+
+__device__ __forceinline__ int dsgn(double v) { return (0.0 < v) - (v < 0.0); }
+
+__global__ void fim_init_kernel(const double* phi, int64_t nx, int64_t ny, double* dist,
+                                unsigned char* fixed) {
+  const int64_t n = nx * ny;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = i % nx, y = i / nx;
+    const double c = phi[i];
+    bool s = false;
+    for (int d = 0; d < 2 && !s; ++d)
+      for (int k = -1; k <= 1 && !s; k += 2) {
+        const int64_t xx = lmir(x + (d == 0 ? k : 0), nx), yy = lmir(y + (d == 1 ? k : 0), ny);
+        const double o = phi[yy * nx + xx];
+        if (dsgn(c) != dsgn(o) && fabs(c) < fabs(o)) s = true;
+      }
+    fixed[i] = s ? 1 : 0;
+    dist[i] = s ? fabs(c) : DBL_MAX;
+  }
+}
+
+__device__ __forceinline__ double eik_local(double xm, double xp, double ym, double yp, double h) {
+  const double a = dmin_(xm, xp), b = dmin_(ym, yp);
+  const double fh = 1.0 * h;
+  const double amb = a - b;
+  if (fabs(amb) >= fh) return dmin_(a, b) + fh;
+  return 0.5 * (a + b + sqrt(2.0 * fh * fh - (amb * amb)));
+}
+
+// One pass over the active tiles: each tile relaxes in shared memory (halo
+// from the previous pass, +max outside the domain) and flags itself and its
+// neighbours for the next pass where anything changed.  Relaxation is
+// monotone (values only decrease), so the result is the unique fixed point
+// whatever the order of updates.
+__global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
+    const double* __restrict__ src, double* __restrict__ dst,
+    const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny, double h,
+    const int* __restrict__ active_in, int* __restrict__ active_out, int tiles_x, int tiles_y,
+    int* __restrict__ any_change) {
+  const int t = blockIdx.x;
+  const int tx0 = t % tiles_x, ty0 = t / tiles_x;
+  const bool active = active_in[t] != 0;
+  const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
+  const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
+  const bool in = x < nx && y < ny;
+  const int64_t i = y * nx + x;
+  if (!active) {
+    if (in) dst[i] = src[i];
+    return;
+  }
+  __shared__ double s[FT + 2][FT + 2];
+  __shared__ int changed;
+  if (threadIdx.x == 0) changed = 0;
+  // interior and halo
+  for (int k = threadIdx.x; k < (FT + 2) * (FT + 2); k += FT * FT) {
+    const int hx = k % (FT + 2), hy = k / (FT + 2);
+    const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
+    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
+  }
+  __syncthreads();
+  const bool free_cell = in && !fixed[i];
+  for (int r = 0; r < FIM_INNER; ++r) {
+    double q = 0.0;
+    if (free_cell)
+      q = eik_local(s[ly + 1][lx], s[ly + 1][lx + 2], s[ly][lx + 1], s[ly + 2][lx + 1], h);
+    __syncthreads();
+    if (free_cell && q < s[ly + 1][lx + 1]) {
+      s[ly + 1][lx + 1] = q;
+      changed = 1;
+    }
+    __syncthreads();
+  }
+  if (in) dst[i] = s[ly + 1][lx + 1];
+  if (threadIdx.x == 0 && changed) {
+    *any_change = 1;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int ax = tx0 + dx, ay = ty0 + dy;
+        if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y) active_out[ay * tiles_x + ax] = 1;
+      }
+  }
+}
+
+__global__ void fim_sign_kernel(const double* phi, double* out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)dsgn(phi[i]) * fabs(out[i]);
+}
+
+__global__ void fill_int_kernel(int* p, int n, int v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+int check_ls_grid(const fl_grid* g) {
+  if (g == nullptr) return set_error(kEInval, "grid is NULL");
+  if (g->dims != 2) return set_error(kEInval, "level-set kernels are 2-D");
+  if (g->n[0] < 4 || g->n[1] < 4 || g->n[2] != 1)
+    return set_error(kEInval, "level-set grid needs n[0], n[1] >= 4 and n[2] = 1");
+  return kOk;
+}
+
+unsigned grid1d(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return (unsigned)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+}  // namespace
+}  // namespace fl
+
+using namespace fl;
+
+extern "C" {
+
+int64_t fl_ls_workspace_bytes(const fl_grid* grid) {
+  if (check_ls_grid(grid) != kOk) return -1;
+  const int64_t n = grid->n[0] * grid->n[1];
+  const int64_t tiles = ((grid->n[0] + FT - 1) / FT) * ((grid->n[1] + FT - 1) / FT);
+  // two FP64 planes (RK3 stages / relaxation ping-pong), fixed-cell flags,
+  // two active-tile lists and a change flag, each 256-byte aligned
+  auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+  return al(2 * n * 8) + al(n) + al(2 * tiles * 4) + 256;
+}
+
+int fl_ls_velocity(const fl_grid* grid, int nmat, const double* const* phis,
+                   const void* const* states, int64_t pitch, uint32_t policy, double h,
+                   double* vel, void* stream) {
+  int rc = check_ls_grid(grid);
+  if (rc) return rc;
+  if (nmat < 1 || nmat > 2) return set_error(kEInval, "nmat must be 1 or 2");
+  if (!phis || !states || !vel) return set_error(kEInval, "NULL pointer");
+  for (int m = 0; m < nmat; ++m)
+    if (!phis[m] || !states[m]) return set_error(kEInval, "NULL material %d", m);
+  if (pitch < grid->n[0] * grid->n[1]) return set_error(kEInval, "pitch below the cell count");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t n = grid->n[0] * grid->n[1];
+  const double* p1 = nmat > 1 ? phis[1] : phis[0];
+  if (policy & 1u) {
+    const float* u1 = static_cast<const float*>(nmat > 1 ? states[1] : states[0]);
+    ls_velocity_kernel<float><<<grid1d(n), 256, 0, st>>>(grid->n[0], grid->n[1], nmat, phis[0], p1,
+                                                         static_cast<const float*>(states[0]), u1,
+                                                         pitch, h, vel);
+  } else {
+    const double* u1 = static_cast<const double*>(nmat > 1 ? states[1] : states[0]);
+    ls_velocity_kernel<double><<<grid1d(n), 256, 0, st>>>(grid->n[0], grid->n[1], nmat, phis[0],
+                                                          p1, static_cast<const double*>(states[0]),
+                                                          u1, pitch, h, vel);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(kECuda, "fl_ls_velocity: %s", cudaGetErrorString(e));
+  return kOk;
+}
+
+int fl_ls_advect(const fl_grid* grid, const double* phi, const double* vel, double dt, double h,
+                 double* out, void* workspace, void* stream) {
+  int rc = check_ls_grid(grid);
+  if (rc) return rc;
+  if (!phi || !vel || !out || !workspace) return set_error(kEInval, "NULL pointer");
+  if (out == phi) return set_error(kEInval, "out must differ from phi");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t nx = grid->n[0], ny = grid->n[1], n = nx * ny;
+  double* s1 = static_cast<double*>(workspace);
+  double* s2 = s1 + n;
+  const dim3 g((unsigned)((nx + LX - 1) / LX), (unsigned)((ny + LY - 1) / LY));
+  ls_rk3_kernel<1><<<g, LX * LY, 0, st>>>(phi, nullptr, vel, dt, h, nx, ny, s1);
+  ls_rk3_kernel<2><<<g, LX * LY, 0, st>>>(phi, s1, vel, dt, h, nx, ny, s2);
+  ls_rk3_kernel<3><<<g, LX * LY, 0, st>>>(phi, s2, vel, dt, h, nx, ny, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(kECuda, "fl_ls_advect: %s", cudaGetErrorString(e));
+  return kOk;
+}
+
+int fl_ls_project(int64_t cells, double* a, double* b, void* stream) {
+  if (cells <= 0 || !a || !b) return set_error(kEInval, "bad arguments");
+  ls_project_kernel<<<grid1d(cells), 256, 0, static_cast<cudaStream_t>(stream)>>>(cells, a, b);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(kECuda, "fl_ls_project: %s", cudaGetErrorString(e));
+  return kOk;
+}
+
+int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, void* workspace,
+                 int max_passes, int* passes, void* stream) {
+  int rc = check_ls_grid(grid);
+  if (rc) return rc;
+  if (!phi || !out || !workspace) return set_error(kEInval, "NULL pointer");
+  if (out == phi) return set_error(kEInval, "out must differ from phi");
+  if (max_passes <= 0) return set_error(kEInval, "max_passes must be positive");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t nx = grid->n[0], ny = grid->n[1], n = nx * ny;
+  const int tiles_x = (int)((nx + FT - 1) / FT), tiles_y = (int)((ny + FT - 1) / FT);
+  const int tiles = tiles_x * tiles_y;
+  auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+  char* w = static_cast<char*>(workspace);
+  double* a = reinterpret_cast<double*>(w);
+  double* b = a + n;
+  unsigned char* fixed = reinterpret_cast<unsigned char*>(w + al(2 * n * 8));
+  int* act0 = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n));
+  int* act1 = act0 + tiles;
+  int* flag = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(2 * tiles * 4));
+  fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, a, fixed);
+  fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(act0, tiles, 1);
+  int pass = 0;
+  int h_flag = 1;
+  cudaError_t e = cudaGetLastError();
+  while (e == cudaSuccess && pass < max_passes && h_flag) {
+    fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(act1, tiles, 0);
+    fill_int_kernel<<<1, 32, 0, st>>>(flag, 1, 0);
+    fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(a, b, fixed, nx, ny, h, act0, act1, tiles_x,
+                                               tiles_y, flag);
+    double* t = a;
+    a = b;
+    b = t;
+    int* ta = act0;
+    act0 = act1;
+    act1 = ta;
+    ++pass;
+    e = cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(out, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    fim_sign_kernel<<<grid1d(n), 256, 0, st>>>(phi, out, n);
+    if (e == cudaSuccess) e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return set_error(kECuda, "fl_ls_reinit: %s", cudaGetErrorString(e));
+  if (passes) *passes = pass;
+  if (h_flag) return set_error(kETimeout, "reinitialisation did not converge in %d passes", pass);
+  return kOk;
+}
+
+}  // extern "C"

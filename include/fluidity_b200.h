@@ -255,6 +255,107 @@ int fl_adj_dtdh(const fl_adj* adj, double* out);
  * checkpoint segment once. */
 int fl_adj_backward(fl_adj* adj, const void* lambda_final, void* lambda_0, void* stream);
 
+/* ---- level sets of the multimaterial (ghost-fluid) path ---------------------
+ * FP64 level sets on 2-D grids (grid->dims == 2), x fastest, one value per
+ * cell; reads outside the domain mirror it.  Each call is asynchronous on
+ * `stream` except fl_ls_reinit, which waits for its convergence flag. */
+
+/* Device workspace fl_ls_advect and fl_ls_reinit need (bytes; -1 on a bad
+ * grid).  The caller allocates it; the calls never allocate. */
+int64_t fl_ls_workspace_bytes(const fl_grid* grid);
+
+/* Interface-normal velocity v = u . grad(phi)/|grad(phi)| of the first of
+ * nmat (1 or 2) materials whose level set is <= 0 at the cell, else 0.
+ * states[m]: the material's SoA state (rho, E, m_x, m_y; FP32 or FP64 by
+ * policy bit 0) with `pitch`.  Replaces the velocity initialisation of
+ * levelset/cuda/velocity_initialization.cuh:108-143 (set_velocities). */
+int fl_ls_velocity(const fl_grid* grid, int nmat, const double* const* phis,
+                   const void* const* states, int64_t pitch, uint32_t policy, double h,
+                   double* vel, void* stream);
+
+/* One TVD-RK3 step of phi_t + vel |grad phi| = 0 (WENO-HJ5 derivatives,
+ * Godunov upwind Hamiltonian), three launches over the whole grid.
+ * Replaces scheme/cuda/evolve.cuh:51-157 with the RK3 updater
+ * (scheme/updaters/runge_kutta_3.hpp:110-148).  out != phi. */
+int fl_ls_advect(const fl_grid* grid, const double* phi, const double* vel, double dt, double h,
+                 double* out, void* workspace, void* stream);
+
+/* a, b <- the two level sets without overlap or void: a -= (a + b) / 2,
+ * b = -a.  Replaces levelset/cuda/levelset_projection.cuh:54-67. */
+int fl_ls_project(int64_t cells, double* a, double* b, void* stream);
+
+/* Reinitialisation to a signed distance (fast iterative method): cells next
+ * to a sign change keep |phi|, every other cell converges to the Godunov
+ * eikonal fixed point, the result takes phi's sign.  Active 16x16 tiles,
+ * at most max_passes passes (FL_ETIMEOUT beyond); *passes (nullable) gets
+ * the count.  Replaces scheme/cuda/fast_iterative_method.cuh:48-112 and its
+ * driver (fast_iterative, :366-); the reference seeds sources with the signed
+ * phi, here with |phi|, so both sides of the interface relax to distances.
+ * out != phi. */
+int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, void* workspace,
+                 int max_passes, int* passes, void* stream);
+
+/* ---- two-material ghost-fluid path ------------------------------------------
+ * Two materials on one 2-D grid, each with its own SoA state (rho, E, m_x,
+ * m_y; FP32 or FP64 by policy bit 0; both with grid->pitch), its own ideal-gas
+ * gamma and an FP64 level set (negative inside).  Replaces the
+ * MultimaterialSimulator step (simulator/multimaterial_simulator.hpp:254-286),
+ * whose own simulate() is not runnable as shipped. */
+typedef struct fl_mm fl_mm;
+
+/* Allocates the workspace (interface lists of grid size, the level-set
+ * workspace, velocities).  gammas: 2 values; res: the cell size dh. */
+int fl_mm_create(fl_mm** mm, const fl_grid* grid, const double* gammas, uint32_t policy,
+                 double res);
+int fl_mm_destroy(fl_mm* mm);
+
+/* Ghost cells of both materials (ghost::load_ghost_cells,
+ * ghost_fluid/cuda/load_ghost_cells.cuh:74-95): RiemannGFM<3> star states
+ * (ghost_fluid/riemann_ghost_fluid.hpp:50-195) written beside the interface,
+ * read from the states as they were before the pass, the highest source
+ * index winning a shared target; then GhostCellExtrapolator
+ * (ghost_fluid/ghost_fluid_extrapolator.hpp:54-202) as Jacobi sweeps over the
+ * band dh <= phi <= 6 dh / sqrt(2) until no cell moves by 1e-8, at most
+ * max_iters sweeps.  scratch0/1: state-sized buffers whose contents are
+ * overwritten in the band. */
+int fl_mm_ghost(fl_mm* mm, void* u0, void* u1, void* scratch0, void* scratch1,
+                const double* phi0, const double* phi1, int max_iters, void* stream);
+
+/* Counters of the last ghost pass and step: [GFM targets of material 0, 1,
+ * band cells 0, 1, extrapolation sweeps 0, 1, reinitialisation passes 0, 1];
+ * n >= 8.  Waits for the device. */
+int fl_mm_stats(const fl_mm* mm, int32_t* out, int32_t n);
+
+/* Cells with phi <= 0 take the conservative form of prim = (rho, p, v_x, v_y)
+ * (state::set_states, state/cuda/state_initialization.cuh:72-119). */
+int fl_mm_set_states(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
+                     const double* prim, double gamma, void* stream);
+
+/* Cells with phi1 <= 0 copy material 1's state into u0
+ * (material::combine_into_first, material/cuda/combine_materials.cuh:39-81). */
+int fl_mm_combine(const fl_grid* grid, uint32_t policy, void* u0, const void* u1,
+                  const double* phi1, void* stream);
+
+/* Step loop.  u0a/u1a hold the states (and hold them again after every
+ * step), u0b/u1b are their second buffers; phi0a/phi1a hold the level sets,
+ * phi0b/phi1b are their second buffers (fl_mm_status says which one is
+ * current).  Level sets are reinitialised after every reinit_every-th step
+ * (0: never; the reference reinitialises every step). */
+int fl_mm_begin(fl_mm* mm, void* u0a, void* u0b, void* u1a, void* u1b, double* phi0a,
+                double* phi0b, double* phi1a, double* phi1b, double cfl, double sim_time,
+                int64_t max_iters, int reinit_every);
+
+/* Runs up to nsteps steps: ghost cells, CFL step over both materials (one
+ * 16-byte read-back per step), each material's split step with its own
+ * gamma, level-set velocity, advection, projection and reinitialisation.
+ * FL_ENAN if a wavespeed is not finite. */
+int fl_mm_steps(fl_mm* mm, int64_t nsteps, void* stream);
+
+/* Waits for the stream; steps, simulated time, done flag and the current
+ * level-set buffers (nullable outputs). */
+int fl_mm_status(fl_mm* mm, void* stream, int64_t* iters, double* run_time, int* done,
+                 double** phi0, double** phi1);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,24 @@ def lib():
         L.flo_extend_f64.argtypes = [P(_Grid), C.c_void_p, C.c_int, C.c_uint32, C.c_void_p]
         L.flo_fill_riemann_f64.argtypes = [P(_Grid), C.c_void_p, C.c_double, C.c_void_p]
         L.flo_fill_riemann_f32.argtypes = [P(_Grid), C.c_void_p, C.c_float, C.c_void_p]
+        L.flo_ls_advect_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_double,
+                                        C.c_double, C.c_void_p]
+        L.flo_ls_velocity_f64.argtypes = [C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_int64, C.c_double, C.c_void_p]
+        L.flo_ls_project_f64.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
+        L.flo_ls_reinit_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
+                                        C.c_void_p, C.c_int]
+        L.flo_ls_reinit_f64.restype = C.c_int
+        L.flo_mm_gfm.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                 C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_int]
+        L.flo_mm_gfm.restype = C.c_int64
+        L.flo_mm_extrapolate.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_void_p,
+                                         C.c_void_p, C.c_int, C.c_int]
+        L.flo_mm_extrapolate.restype = C.c_int
+        L.flo_mm_set_states.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_int]
+        L.flo_mm_combine.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -296,3 +314,120 @@ def ref_simulate(shape, u, gamma, cfl, res, sim_time, max_iters, flux="hllc",
     if steps < 0:
         raise ValueError("reference simulate failed")
     return (b if in_b.value else a), int(steps), rt.value, dts[:min(steps, cap)]
+
+
+# ---- level set (FP64, 2-D; arrays are (cells,) with x fastest) -------------
+
+def ls_advect(nx, ny, phi, vel, dt, h):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    out = np.empty_like(phi)
+    lib().flo_ls_advect_f64(nx, ny, _ptr(phi), _ptr(vel), dt, h, _ptr(out))
+    return out
+
+
+def ls_velocity(nx, ny, phis, states, h):
+    """phis: list of (cells,) level sets; states: list of (4, pitch) states."""
+    phis = [np.ascontiguousarray(p, dtype=np.float64) for p in phis]
+    states = [np.ascontiguousarray(s, dtype=np.float64) for s in states]
+    pitch = states[0].shape[1]
+    pp = (C.c_void_p * len(phis))(*[p.ctypes.data for p in phis])
+    sp = (C.c_void_p * len(states))(*[s.ctypes.data for s in states])
+    out = np.empty(nx * ny, dtype=np.float64)
+    lib().flo_ls_velocity_f64(nx, ny, len(phis), pp, sp, pitch, h, _ptr(out))
+    return out
+
+
+def ls_project(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64).copy()
+    b = np.ascontiguousarray(b, dtype=np.float64).copy()
+    lib().flo_ls_project_f64(a.size, _ptr(a), _ptr(b))
+    return a, b
+
+
+def ls_reinit(nx, ny, phi, h, max_sweeps=100000):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    out = np.empty_like(phi)
+    sweeps = lib().flo_ls_reinit_f64(nx, ny, _ptr(phi), h, _ptr(out), max_sweeps)
+    return out, sweeps
+
+
+# ---- two-material ghost-fluid path (fl_mm_oracle.c) ---------------------------
+# States: (4, pitch) arrays, float64 or float32 (FP32 values are carried as
+# doubles in the C code and rounded back to float on every store).
+
+def _as_f64(u):
+    return np.ascontiguousarray(u, dtype=np.float64).copy()
+
+
+def mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1):
+    """Riemann ghost-fluid star states for both materials; returns (u0, u1, n)."""
+    f32 = u0.dtype == np.float32
+    a, b = _as_f64(u0), _as_f64(u1)
+    p0 = np.ascontiguousarray(phi0, dtype=np.float64)
+    p1 = np.ascontiguousarray(phi1, dtype=np.float64)
+    n = lib().flo_mm_gfm(nx, ny, a.shape[1], h, gammas[0], gammas[1], _ptr(a), _ptr(b), _ptr(p0),
+                         _ptr(p1), int(f32))
+    dt = np.float32 if f32 else np.float64
+    return a.astype(dt), b.astype(dt), int(n)
+
+
+def mm_extrapolate(nx, ny, h, u, phi, max_iters=64):
+    """Ghost-cell extrapolation of one material; returns (u, sweeps)."""
+    f32 = u.dtype == np.float32
+    a = _as_f64(u)
+    p = np.ascontiguousarray(phi, dtype=np.float64)
+    it = lib().flo_mm_extrapolate(nx, ny, a.shape[1], h, _ptr(a), _ptr(p), int(f32), max_iters)
+    return a.astype(u.dtype), int(it)
+
+
+def mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters=64):
+    """GFM for both materials, then the extrapolation of each."""
+    u0, u1, _ = mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1)
+    u0, _ = mm_extrapolate(nx, ny, h, u0, phi0, max_iters)
+    u1, _ = mm_extrapolate(nx, ny, h, u1, phi1, max_iters)
+    return u0, u1
+
+
+def mm_set_states(u, phi, prim, gamma):
+    f32 = u.dtype == np.float32
+    a = _as_f64(u)
+    p = np.ascontiguousarray(phi, dtype=np.float64)
+    pr = np.ascontiguousarray(prim, dtype=np.float64)
+    lib().flo_mm_set_states(p.size, a.shape[1], _ptr(a), _ptr(p), _ptr(pr), gamma, int(f32))
+    return a.astype(u.dtype)
+
+
+def mm_combine(u0, u1, phi1):
+    a = _as_f64(u0)
+    b = _as_f64(u1)
+    p = np.ascontiguousarray(phi1, dtype=np.float64)
+    lib().flo_mm_combine(p.size, a.shape[1], _ptr(a), _ptr(b), _ptr(p))
+    return a.astype(u0.dtype)
+
+
+def mm_step(nx, ny, h, gammas, cfl, u0, u1, phi0, phi1, reinit, max_iters=64):
+    """One step of the two-material loop: ghost cells, CFL time step over
+    both materials, split MUSCL-Hancock/HLLC step of each material with its
+    own gamma, level-set velocity, RK3 advection, projection and (when
+    reinit) reinitialisation of both level sets.  Returns
+    (u0, u1, phi0, phi1, dt)."""
+    shape = (nx, ny)
+    u0, u1 = mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters)
+    ws = max(float(max_wavespeed(shape, u0, gammas[0])), float(max_wavespeed(shape, u1, gammas[1])))
+    dt = cfl * h / ws
+    dtdh = dt / h
+    out = []
+    for u, g in ((u0, gammas[0]), (u1, gammas[1])):
+        v = sweep(shape, 0, u, g, dtdh)
+        v = sweep(shape, 1, v, g, dtdh)
+        out.append(v)
+    u0, u1 = out
+    vel = ls_velocity(nx, ny, [phi0, phi1], [u0.astype(np.float64), u1.astype(np.float64)], h)
+    a = ls_advect(nx, ny, phi0, vel, dt, h)
+    b = ls_advect(nx, ny, phi1, vel, dt, h)
+    a, b = ls_project(a, b)
+    if reinit:
+        a, _ = ls_reinit(nx, ny, a, h)
+        b, _ = ls_reinit(nx, ny, b, h)
+    return u0, u1, a, b, dt
