@@ -16,9 +16,10 @@
 //    interface keep |phi| (scheme/cuda/fast_iterative_method.cuh:48-89, which
 //    seeds the signed value), every other cell
 //    relaxes to the fixed point of the Godunov local eikonal solve
-//    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles iterate in shared
-//    memory and only tiles next to a change run the next pass (active-tile
-//    list); the result takes the input's sign (set_signs, :96-112).
+//    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles relax in shared
+//    memory and in place, only tiles stamped by a changed neighbour run the
+//    next pass, and the host checks convergence once per 16 passes; the
+//    result takes the input's sign (set_signs, :96-112).
 // FP64 level sets on 2-D grids; out-of-domain reads mirror the domain.
 #include <cuda_runtime.h>
 
@@ -192,38 +193,41 @@ __device__ __forceinline__ double eik_local(double xm, double xp, double ym, dou
   return 0.5 * (a + b + sqrt(2.0 * fh * fh - (amb * amb)));
 }
 
-// One pass over the active tiles: each tile relaxes in shared memory (halo
-// from the previous pass, +max outside the domain) and flags itself and its
-// neighbours for the next pass where anything changed.  Relaxation is
-// monotone (values only decrease), so the result is the unique fixed point
-// whatever the order of updates.
+// Pass k over the tiles, in place on d.  A tile runs in pass 0 and in every
+// pass whose number its stamp has reached (a changed tile stamps itself and
+// its eight neighbours with k + 1).  It loads itself and a one-cell halo (+max
+// outside the domain), relaxes FIM_INNER rounds in shared memory and writes
+// back.  Neighbouring tiles may update their cells while this tile reads its
+// halo; every value read is then either the old or the new one, both upper
+// bounds of the fixed point, and since each update only lowers a value
+// through a monotone local solve, the relaxation reaches the same fixed point
+// whatever the interleaving.  A pass after one that changed nothing returns
+// at once (last_change < k - 1).
 __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
-    const double* __restrict__ src, double* __restrict__ dst,
-    const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny, double h,
-    const int* __restrict__ active_in, int* __restrict__ active_out, int tiles_x, int tiles_y,
-    int* __restrict__ any_change) {
+    double* __restrict__ d, const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny,
+    double h, int* __restrict__ stamp, int tiles_x, int tiles_y, int* __restrict__ last_change,
+    int k) {
+  if (k > 0 && *(volatile int*)last_change < k - 1) return;
   const int t = blockIdx.x;
+  if (k > 0 && *(volatile int*)(stamp + t) < k) return;
   const int tx0 = t % tiles_x, ty0 = t / tiles_x;
-  const bool active = active_in[t] != 0;
   const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
   const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
   const bool in = x < nx && y < ny;
   const int64_t i = y * nx + x;
-  if (!active) {
-    if (in) dst[i] = src[i];
-    return;
-  }
   __shared__ double s[FT + 2][FT + 2];
   __shared__ int changed;
   if (threadIdx.x == 0) changed = 0;
-  // interior and halo
-  for (int k = threadIdx.x; k < (FT + 2) * (FT + 2); k += FT * FT) {
-    const int hx = k % (FT + 2), hy = k / (FT + 2);
+  for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
+    const int hx = q % (FT + 2), hy = q / (FT + 2);
     const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
-    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
+    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
+                    ? *(volatile const double*)(d + gy * nx + gx)
+                    : DBL_MAX;
   }
   __syncthreads();
   const bool free_cell = in && !fixed[i];
+  bool mine = false;
   for (int r = 0; r < FIM_INNER; ++r) {
     double q = 0.0;
     if (free_cell)
@@ -231,17 +235,21 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     __syncthreads();
     if (free_cell && q < s[ly + 1][lx + 1]) {
       s[ly + 1][lx + 1] = q;
-      changed = 1;
+      mine = true;
     }
     __syncthreads();
   }
-  if (in) dst[i] = s[ly + 1][lx + 1];
+  if (mine) {
+    d[i] = s[ly + 1][lx + 1];
+    changed = 1;
+  }
+  __syncthreads();
   if (threadIdx.x == 0 && changed) {
-    *any_change = 1;
+    atomicMax(last_change, k);
     for (int dy = -1; dy <= 1; ++dy)
       for (int dx = -1; dx <= 1; ++dx) {
         const int ax = tx0 + dx, ay = ty0 + dy;
-        if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y) active_out[ay * tiles_x + ax] = 1;
+        if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y) stamp[ay * tiles_x + ax] = k + 1;
       }
   }
 }
@@ -280,8 +288,9 @@ int64_t fl_ls_workspace_bytes(const fl_grid* grid) {
   if (check_ls_grid(grid) != kOk) return -1;
   const int64_t n = grid->n[0] * grid->n[1];
   const int64_t tiles = ((grid->n[0] + FT - 1) / FT) * ((grid->n[1] + FT - 1) / FT);
-  // two FP64 planes (RK3 stages / relaxation ping-pong), fixed-cell flags,
-  // two active-tile lists and a change flag, each 256-byte aligned
+  // two FP64 planes (RK3 stages), fixed-cell flags of the reinitialisation,
+  // its tile stamps (room for two ints per tile) and its change counter,
+  // each 256-byte aligned
   auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
   return al(2 * n * 8) + al(n) + al(2 * tiles * 4) + 256;
 }
@@ -355,40 +364,39 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
   const int tiles = tiles_x * tiles_y;
   auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
   char* w = static_cast<char*>(workspace);
-  double* a = reinterpret_cast<double*>(w);
-  double* b = a + n;
   unsigned char* fixed = reinterpret_cast<unsigned char*>(w + al(2 * n * 8));
-  int* act0 = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n));
-  int* act1 = act0 + tiles;
-  int* flag = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(2 * tiles * 4));
-  fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, a, fixed);
-  fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(act0, tiles, 1);
-  int pass = 0;
-  int h_flag = 1;
+  int* stamp = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n));
+  int* last = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(2 * tiles * 4));
+  // the relaxation runs in place in `out`
+  fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, out, fixed);
+  fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(stamp, tiles, 0);
+  fill_int_kernel<<<1, 32, 0, st>>>(last, 1, 0);
+  // passes are launched in chunks; the host reads the last pass that changed
+  // anything after each chunk (passes past convergence return at once)
+  constexpr int CHUNK = 16;
+  int launched = 0, h_last = 0;
+  bool converged = false;
   cudaError_t e = cudaGetLastError();
-  while (e == cudaSuccess && pass < max_passes && h_flag) {
-    fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(act1, tiles, 0);
-    fill_int_kernel<<<1, 32, 0, st>>>(flag, 1, 0);
-    fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(a, b, fixed, nx, ny, h, act0, act1, tiles_x,
-                                               tiles_y, flag);
-    double* t = a;
-    a = b;
-    b = t;
-    int* ta = act0;
-    act0 = act1;
-    act1 = ta;
-    ++pass;
-    e = cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  while (e == cudaSuccess && !converged && launched < max_passes) {
+    const int end = launched + CHUNK < max_passes ? launched + CHUNK : max_passes;
+    for (int k = launched; k < end; ++k)
+      fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(out, fixed, nx, ny, h, stamp, tiles_x, tiles_y,
+                                                 last, k);
+    launched = end;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_last, last, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    // converged once a pass after the last change has run
+    converged = (e == cudaSuccess) && (h_last + 1 < launched);
   }
   if (e == cudaSuccess) {
-    e = cudaMemcpyAsync(out, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st);
     fim_sign_kernel<<<grid1d(n), 256, 0, st>>>(phi, out, n);
-    if (e == cudaSuccess) e = cudaGetLastError();
+    e = cudaGetLastError();
   }
   if (e != cudaSuccess) return set_error(kECuda, "fl_ls_reinit: %s", cudaGetErrorString(e));
-  if (passes) *passes = pass;
-  if (h_flag) return set_error(kETimeout, "reinitialisation did not converge in %d passes", pass);
+  if (passes) *passes = converged ? h_last + 2 : launched;
+  if (!converged)
+    return set_error(kETimeout, "reinitialisation did not converge in %d passes", launched);
   return kOk;
 }
 
