@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 
 GAMMA = 1.4
 SEED = 0
+# DRAM bytes (read + write) per cell of one sweep launch, from the ncu
+# capture of the 2048^2 FP64 HLLC case (walk_kernel_2d, x and y sweeps
+# averaged: 241.5 MB per launch over 2048^2 cells); traffic grows with the
+# cell count, so the bench scales it to its own grid.
+MEASURED_TRAFFIC_PER_CELL = {("f64", "hllc"): 57.6}
 
 
 def parse():
@@ -52,6 +57,10 @@ def parse():
     p.add_argument("--no-variants", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-mm", action="store_true")
+    p.add_argument("--mm-steps", type=int, default=500)
+    p.add_argument("--only", choices=["mm", "adjoint", "batched"], default=None,
+                   help="run one secondary workload alone (profiling); prints its own line")
     return p.parse_args()
 
 
@@ -348,8 +357,12 @@ def run_ours(a, world, rank, local):
         "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
         "config": workload_config(a),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "kernel": "sweep_kernel (x and y sweeps, averaged)",
+                     "frac": achieved / peak,
+                     "traffic": (MEASURED_TRAFFIC_PER_CELL[(a.dtype, a.flux)] * cells
+                                 if (a.dtype, a.flux) in MEASURED_TRAFFIC_PER_CELL else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                       "2048^2 capture, per cell, scaled to this grid",
+                     "kernel": "walk_kernel_2d (x and y sweeps, averaged)",
                      "algorithmic_bytes_per_launch": bytes_per_sweep,
                      "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
@@ -363,6 +376,9 @@ def run_ours(a, world, rank, local):
         line["batched"] = measure_batched()
     if rank == 0 and world == 1 and not a.no_adjoint:
         line["adjoint"] = measure_adjoint()
+    if rank == 0 and world == 1 and not a.no_mm:
+        line["multimaterial"] = measure_multimaterial(steps=a.mm_steps,
+                                                      cpu=not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(a)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores,
@@ -469,16 +485,52 @@ def measure_batched(seed=3, steps=200, baseline_every=4):
     }
 
 
-def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
-    """Gradient workload: 2-D n x n, density 1 + 32 seeded Gaussians, p = 1,
-    at rest; 300 HLLC/MUSCL steps at CFL 0.7; J = 0.5 ||p(T) - p_target||^2
-    with p_target from a second seed's field; dJ/d rho0 by the discrete
-    adjoint with ceil(sqrt(300)) = 18-step checkpoints, checked against
-    central differences along seeded unit directions (time steps frozen)."""
+def _fd_check(adj, rho0, grad, p_target, directions, eps, seed=7):
+    """Relative mismatch, per seeded unit direction, of central differences
+    (time steps frozen from the unperturbed forward pass) against the
+    adjoint's directional derivative; NaN where a value is not finite."""
     import torch
-    from fluidity_b200.adjoint import (Adjoint, gaussian_density, objective, pressure,
-                                       random_directions, rollout, state_from_density)
+    from fluidity_b200.adjoint import objective, random_directions, state_from_density
+    dts = adj.dtdh()
+    out = []
+    with torch.no_grad():
+        for v in random_directions(rho0.numel(), directions, seed=seed, dtype=rho0.dtype):
+            jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7,
+                                       frozen_dtdh=dts), p_target).item()
+            jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7,
+                                       frozen_dtdh=dts), p_target).item()
+            fd = (jp - jm) / (2 * eps)
+            ad = torch.dot(grad, v).item()
+            r = abs(fd - ad) / max(abs(ad), 1e-300)
+            out.append(r if math.isfinite(r) else float("nan"))
+    return out
+
+
+def _fd_summary(errs):
+    finite = [e for e in errs if math.isfinite(e)]
+    return {"max": max(finite) if len(finite) == len(errs) else float("nan"),
+            "median": statistics.median(finite) if finite else float("nan"),
+            "below_1e-6": sum(1 for e in finite if e < 1e-6),
+            "per_direction": [float(f"{e:.3g}") for e in errs]}
+
+
+def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
+    """Gradient workload: 2-D n x n, density 1 + 32 seeded Gaussians at rest
+    with p = rho (temperature 1; with a uniform p the field is an exact steady
+    state and the objective would not depend on the density); 300 HLLC/MUSCL
+    steps at CFL 0.7; J = 0.5 ||p(T) - p_target||^2 with p_target from a
+    second seed's field; dJ/d rho0 by the discrete adjoint with
+    ceil(sqrt(300)) = 18-step checkpoints, checked against central differences
+    along 16 seeded unit directions (time steps frozen) at eps 1e-6 and 1e-7.
+    The discrete step is piecewise smooth (minmod switches, the HLLC
+    shock/rarefaction estimate): a direction whose central difference
+    straddles a switch mixes two one-sided derivatives, so the check reports
+    every direction, not only the worst."""
+    import torch
+    from fluidity_b200.adjoint import (Adjoint, gaussian_density, objective, pressure, rollout,
+                                       state_from_density)
     out = {}
+    grads = {}
     for dtype in ("f64", "f32"):
         tdt = torch.float64 if dtype == "f64" else torch.float32
         adj = Adjoint((n, n), steps, dtype=dtype)
@@ -486,11 +538,11 @@ def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
             p_target = pressure(adj.forward(state_from_density(
                 gaussian_density(n, 2, dtype=tdt)), 0.7))
         rho0 = gaussian_density(n, 1, dtype=tdt).requires_grad_(True)
-        u0 = state_from_density(rho0)
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        uN = rollout(u0, adj, 0.7)            # warm-up (kernel set-up)
+        uN = rollout(state_from_density(rho0), adj, 0.7)   # warm-up (kernel set-up)
         objective(uN, p_target).backward()
         rho0.grad = None
+        u0 = state_from_density(rho0)
         torch.cuda.synchronize()
         e[0].record()
         uN = rollout(u0, adj, 0.7)
@@ -502,31 +554,102 @@ def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
         fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
         grad = rho0.grad.detach().clone()
         res = {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
-               "cost_ratio_backward_over_forward": bwd_ms / fwd_ms}
+               "cost_ratio_backward_over_forward": bwd_ms / fwd_ms,
+               "objective": J.item(), "grad_norm": torch.norm(grad.double()).item()}
+        grads[dtype] = grad.double()
         if dtype == "f64":
-            dts = adj.dtdh()
-            worst = 0.0
-            with torch.no_grad():
-                for v in random_directions(n * n, directions, seed=7):
-                    jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7,
-                                               frozen_dtdh=dts), p_target).item()
-                    jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7,
-                                               frozen_dtdh=dts), p_target).item()
-                    fd = (jp - jm) / (2 * eps)
-                    ad = torch.dot(grad, v).item()
-                    worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-300))
-            res.update({"fd_directions": directions, "fd_eps": eps,
-                        "fd_max_rel_err": worst})
-            out["grad_f64"] = grad
+            e6 = _fd_check(adj, rho0.detach(), grad, p_target, directions, eps)
+            e7 = _fd_check(adj, rho0.detach(), grad, p_target, directions, eps / 10)
+            res.update({"fd_directions": directions,
+                        "fd_eps_1e-6": _fd_summary(e6), "fd_eps_1e-7": _fd_summary(e7),
+                        "fd_max_rel_err": max(e6)})
         else:
-            g64 = out.pop("grad_f64")
-            res["rel_diff_vs_f64_gradient"] = (torch.norm(grad.double() - g64) /
+            g64 = grads["f64"]
+            res["rel_diff_vs_f64_gradient"] = (torch.norm(grads["f32"] - g64) /
                                                torch.norm(g64)).item()
         out[dtype] = res
-    out.pop("grad_f64", None)
-    out["workload"] = (f"2-D {n}x{n}, rho0 = 1 + 32 Gaussians, p = 1, at rest, {steps} HLLC "
-                       f"steps at CFL 0.7, checkpoint every {math.ceil(math.sqrt(steps))} steps")
+    out["workload"] = (f"2-D {n}x{n}, rho0 = 1 + 32 Gaussians, p = rho0, at rest, {steps} "
+                       f"HLLC/MUSCL steps at CFL 0.7, checkpoint every "
+                       f"{math.ceil(math.sqrt(steps))} steps")
     return out
+
+
+def measure_multimaterial(nx=2048, ny=1024, steps=500, reinit_every=5, cpu=True):
+    """Two-material shock-bubble workload: 2048 x 1024 on [0,2] x [0,1]
+    (h = 1/1024), ambient gamma 1.4 shocked at x = 0.1, bubble gamma 1.67,
+    FP32 states, FP64 level sets, HLLC + van Leer MUSCL-Hancock, CFL 0.6,
+    WENO-HJ5/RK3 level-set advection, reinitialisation every 5 steps."""
+    import torch
+    from fluidity_b200.multimaterial import MultiMaterial
+    from fluidity_b200.workloads import shock_bubble
+    spec = shock_bubble(SEED + 1, nx=nx, ny=ny, width=2.0)
+    warm = MultiMaterial.shock_bubble(spec, dtype="f32")
+    warm.begin(0.6, 1e30, 3, reinit_every)
+    warm.steps(3)
+    warm.status()
+    del warm
+    mm = MultiMaterial.shock_bubble(spec, dtype="f32")
+    torch.cuda.synchronize()
+    mm.begin(0.6, 1e30, steps, reinit_every)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    mm.steps(steps)
+    e1.record()
+    it, rt, done = mm.status()
+    ms = e0.elapsed_time(e1)
+    st = mm.stats()
+    u0, u1 = mm.states()
+    p0, _ = mm.current_phi()
+    finite = bool(torch.isfinite(u0).all().item() and torch.isfinite(u1).all().item())
+    cells = nx * ny
+    out = {
+        "workload": f"2-D two-material shock-bubble {nx}x{ny} on [0,2]x[0,1], Mach "
+                    f"{spec['mach']:.3f}, bubble r {spec['radius']:.3f}, FP32 states, FP64 "
+                    f"level sets, HLLC + van Leer, CFL 0.6, reinit every {reinit_every} steps",
+        "steps": it, "simulated_time": rt, "ms": ms, "ms_per_step": ms / max(it, 1),
+        "cell_updates_per_s": cells * it / (ms * 1e-3),
+        "material_cell_updates_per_s": 2 * cells * it / (ms * 1e-3),
+        "last_step": st, "states_finite": finite,
+        "levelset_finite": bool(torch.isfinite(p0).all().item()),
+        "levelset_cells_inside_bubble": int((p0 > 0).sum().item()),
+    }
+    if cpu:
+        import time as _t
+        import numpy as np
+        from oracle import oracle as O
+        g0, g1 = spec["gammas"]
+        n = cells
+        a0 = O.mm_set_states(np.zeros((4, n), np.float32), -np.ones(n), spec["ambient"], g0)
+        a0 = O.mm_set_states(a0, spec["shock_phi"], spec["shocked"], g0)
+        a1 = O.mm_set_states(np.zeros((4, n), np.float32), -np.ones(n), spec["bubble"], g1)
+        p0h, p1h = spec["phi0"], spec["phi1"]
+        t0 = _t.perf_counter()
+        k = 0
+        while k < 2:
+            a0, a1, p0h, p1h, _ = O.mm_step(nx, ny, spec["h"], spec["gammas"], 0.6, a0, a1, p0h,
+                                            p1h, reinit=False)
+            k += 1
+        sec = _t.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cells * k / sec, "unit": "cell-updates/s", "cores": 1,
+                               "kind": "port",
+                               "sample": f"{k} steps (no reinitialisation) of the same "
+                                         f"workload in the C oracle, 1 thread, {sec:.1f} s"}
+    return out
+
+
+def run_section(a, local):
+    """One secondary workload on its own (for profiling captures)."""
+    import torch
+    from fluidity_b200 import build as fb
+    fb.build()
+    torch.cuda.set_device(local)
+    if a.only == "mm":
+        res = measure_multimaterial(steps=a.mm_steps, cpu=not a.no_cpu_baseline)
+    elif a.only == "adjoint":
+        res = measure_adjoint()
+    else:
+        res = measure_batched()
+    print(json.dumps({"section": a.only, **res}), flush=True)
 
 
 def main():
@@ -535,6 +658,8 @@ def main():
     try:
         if a.impl == "reference":
             run_reference_arm(a, world, rank)
+        elif a.only is not None:
+            run_section(a, local)
         else:
             run_ours(a, world, rank, local)
     finally:

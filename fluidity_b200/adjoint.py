@@ -22,12 +22,12 @@ class Adjoint:
     """Checkpointed forward / backward of nsteps steps on one grid."""
 
     def __init__(self, shape, nsteps, dtype="f64", flux="hllc", gamma=1.4, boundary_mask=0,
-                 interval=0):
+                 interval=0, flatten=True, recon="muscl"):
         self.lib = capi.load()
         self.shape = tuple(int(v) for v in shape)
         self.nsteps = int(nsteps)
         self.gamma = float(gamma)
-        self.policy = capi.policy_bits(dtype, flux)
+        self.policy = capi.policy_bits(dtype, flux, recon=recon, flatten=flatten)
         self.grid = capi.Grid.make(self.shape)
         self.dtype = torch.float64 if dtype == "f64" else torch.float32
         h = C.c_void_p()
@@ -117,9 +117,13 @@ def gaussian_density(n: int, seed: int, count: int = 32, device="cuda",
     return rho
 
 
-def state_from_density(rho, gamma=1.4, p=1.0):
-    """Conservative state at rest with pressure p: [rho, p/(gamma-1), 0, 0]."""
-    E = torch.full_like(rho, p / (gamma - 1.0))
+def state_from_density(rho, gamma=1.4, temperature=1.0):
+    """Conservative state at rest with p = rho * temperature:
+    [rho, rho * temperature / (gamma - 1), 0, 0].  (A uniform pressure at rest
+    would be an exact steady state -- every cell a stationary contact, which
+    MUSCL-Hancock with HLLC keeps exactly -- so nothing would move and a
+    pressure objective would not depend on the density.)"""
+    E = rho * (temperature / (gamma - 1.0))
     z = torch.zeros_like(rho)
     return torch.stack([rho, E, z, z])
 
