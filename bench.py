@@ -12,9 +12,11 @@ in HBM when timing starts; each 537 MB state buffer exceeds the 126 MB L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Under torchrun each rank solves its own replica of the workload (the path
-runs independent problems; no collective on the data path) and the line
-reports the aggregate over ranks, timed as the max over ranks.
+Under torchrun (N > 1) the ranks solve one grid of size x (size * N) cells,
+split into N slabs of rows (each GPU keeps a size^2 slab: weak scaling); 4
+ghost rows are exchanged with the neighbouring ranks over NCCL before every
+sweep and the CFL maximum is MAX-reduced once per step.  The line reports the
+aggregate over ranks, timed as the max over ranks.
 """
 from __future__ import annotations
 
@@ -637,6 +639,122 @@ def measure_multimaterial(nx=2048, ny=1024, steps=500, reinit_every=5, cpu=True)
     return out
 
 
+def run_slabs(a, world, rank, local):
+    """N > 1: one 2-D grid of a.size x (a.size * N) cells split into N slabs
+    of rows, one per GPU (weak scaling: each GPU keeps an a.size^2 slab).
+    Before each sweep the ranks exchange 4 ghost rows with their neighbours
+    over NCCL; the CFL maximum is MAX-reduced once per step."""
+    import torch
+    from fluidity_b200 import build as fb
+    fb.build()
+    from fluidity_b200.slab import CudaSlabOps, SlabLayout, SlabRunner
+    from fluidity_b200.solver import SplitSolver
+    from fluidity_b200.workloads import riemann_states
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nx, ny = a.size, a.size * world
+    T = a.time_steps
+    L = SlabLayout((nx, ny), world, rank)
+    ops = CudaSlabOps(L, dtype=a.dtype, flux=a.flux, gamma=GAMMA)
+    runner = SlabRunner(L, ops)
+    buf_a, buf_b = ops.new_state(), ops.new_state()
+    glob = SplitSolver((nx, ny), dtype=a.dtype, flux=a.flux, limiter="vanleer", gamma=GAMMA)
+    init = glob.fill_riemann(riemann_states(SEED, 2))[:, L.global_slice()].contiguous()
+    del glob
+    torch.cuda.empty_cache()
+    stream = torch.cuda.current_stream()
+    res = 1.0 / nx
+
+    def one_run(events=None):
+        buf_a.copy_(init)
+        runner.begin(buf_a, buf_b, 0.8, res, 1e30, T)
+        if events is not None:
+            events[0].record(stream)
+        runner.steps(T)
+        if events is not None:
+            events[1].record(stream)
+
+    for _ in range(a.warmup):
+        one_run()
+    it, _, _, _ = ops.status()
+    if it != T:
+        raise RuntimeError(f"warm-up run stopped after {it} of {T} steps")
+    sampler = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(a.steps):
+        one_run(ev[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    elapsed_ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
+    loop_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev), world, dev)
+    it, _, _, _ = ops.status()
+    if it != T:
+        raise RuntimeError(f"timed run stopped after {it} of {T} steps")
+    value = nx * ny * T * a.steps / (elapsed_ms / 1e3)
+    elem = 8 if a.dtype == "f64" else 4
+    sweep_s = loop_ms / 1e3 / (a.steps * 2 * T)
+    bytes_per_sweep = 2 * 4 * elem * L.cells
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = ((json.load(open(peaks_path))["hbm_gbs"], "measured")
+                      if os.path.exists(peaks_path) else (6650.0, "fallback"))
+    achieved = bytes_per_sweep / sweep_s / 1e9
+
+    # end to end: the slab from pinned host memory, the run, the slab back
+    pin_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
+    pin_out = torch.empty_like(pin_in)
+    pin_in.copy_(init)
+    e2e_steps = max(2, min(a.steps, 5))
+
+    def e2e_run():
+        buf_a.copy_(pin_in, non_blocking=True)
+        runner.begin(buf_a, buf_b, 0.8, res, 1e30, T)
+        runner.steps(T)
+        pin_out.copy_(buf_a, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_run()
+    barrier(world)
+    ts = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_run()
+    e2e_s = max_over_ranks(time.perf_counter() - ts, world, dev)
+    state_bytes = int(buf_a.numel()) * elem
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
+            "config": {**workload_config(a),
+                       "workload": f"2-D four-quadrant Riemann problem {nx}x{ny} ({nx}^2 per "
+                                   f"GPU), {T} steps, MUSCL-Hancock + van Leer + flattening, "
+                                   f"{a.flux.upper()} flux, CFL 0.8, transmissive; {world} "
+                                   f"slabs of rows, 4 ghost rows exchanged before each sweep",
+                       "grid": [nx, ny], "parallelism": f"slab{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "walk_kernel_2d per rank, time per sweep including the "
+                                   "ghost-row exchange and the CFL all-reduce",
+                         "algorithmic_bytes_per_launch": bytes_per_sweep,
+                         "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
+            "e2e": {"value": nx * ny * T * e2e_steps / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes * world,
+                    "d2h_bytes_per_step": state_bytes * world},
+            "gpu_launches": a.steps * (3 * T + 3),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_section(a, local):
     """One secondary workload on its own (for profiling captures)."""
     import torch
@@ -660,6 +778,8 @@ def main():
             run_reference_arm(a, world, rank)
         elif a.only is not None:
             run_section(a, local)
+        elif world > 1:
+            run_slabs(a, world, rank, local)
         else:
             run_ours(a, world, rank, local)
     finally:

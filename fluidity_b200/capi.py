@@ -90,6 +90,11 @@ PROTOTYPES = {
     "fl_sim_destroy": (C.c_int, [_P]),
     "fl_sim_begin": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P]),
     "fl_sim_steps": (C.c_int, [_P, C.c_int64, _P]),
+    "fl_sim_set_rows": (C.c_int, [_P, C.c_int64, C.c_int64]),
+    "fl_sim_set_external_reduce": (C.c_int, [_P, C.c_int]),
+    "fl_sim_set_ws_word": (C.c_int, [_P, _P]),
+    "fl_sim_sweep": (C.c_int, [_P, C.c_int, _P]),
+    "fl_sim_finalize": (C.c_int, [_P, C.c_int, _P]),
     "fl_sim_status": (C.c_int, [_P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int), C.POINTER(_P)]),
     "fl_simulate": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P,

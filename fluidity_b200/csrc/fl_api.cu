@@ -233,6 +233,18 @@ cudaError_t launch_layout(const fl_grid* g, const void* src, void* dst, int to_s
 
 // ---- time control ----------------------------------------------------------
 
+// Takes the reduced max wavespeed from `word` (when given; it is then reset
+// for the next accumulation) and finalises the step.
+__global__ void finalize_kernel(StepControl* c, unsigned long long* word, int advance) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (word != nullptr) {
+      c->ws_bits = *word;
+      *word = 0ull;
+    }
+    if (!c->done) finalize_control(c, advance != 0);
+  }
+}
+
 __global__ void init_control_kernel(StepControl* c, double cfl, double res, double sim_time,
                                     long long max_iters, int is_f32) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -266,6 +278,10 @@ struct fl_sim {
   void* a;
   void* b;
   int64_t enqueued;        // steps enqueued since fl_sim_begin
+  int64_t own_lo, own_hi;  // rows (slowest index) counted in wavespeeds; all if hi <= lo
+  int external;            // 1: the host reduces the wavespeed word and calls fl_sim_finalize
+  unsigned long long* ws_word;  // external: the caller's device word (else ctrl->ws_bits)
+  int cursor;              // next sweep of the current step (fl_sim_sweep)
 };
 
 using namespace fl;
@@ -434,9 +450,27 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res, double s
                                         sim->pol.f32 ? 1 : 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
-  auto* acc = &sim->ctrl->ws_bits;
-  e = sim->pol.f32 ? launch_wavespeed<float>(&sim->grid, a, sim->gamma, acc, sim->ctrl, st)
-                   : launch_wavespeed<double>(&sim->grid, a, sim->gamma, acc, sim->ctrl, st);
+  sim->cursor = 0;
+  if (sim->external && sim->ws_word == nullptr)
+    return fail(kEInval, "external reduction needs fl_sim_set_ws_word");
+  auto* acc = sim->external ? sim->ws_word : &sim->ctrl->ws_bits;
+  if (sim->external) {
+    e = cudaMemsetAsync(acc, 0, sizeof(*acc), st);
+    if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
+  }
+  // own rows only: a view of the grid that starts at row own_lo
+  fl_grid view = sim->grid;
+  const void* base = a;
+  if (sim->own_hi > sim->own_lo) {
+    const int slow = sim->grid.dims - 1;
+    int64_t row_cells = 1;
+    for (int d = 0; d < slow; ++d) row_cells *= sim->grid.n[d];
+    view.n[slow] = sim->own_hi - sim->own_lo;
+    base = static_cast<const char*>(a) + sim->own_lo * row_cells * (int64_t)elem_size(sim->pol);
+  }
+  StepControl* fin = sim->external ? nullptr : sim->ctrl;
+  e = sim->pol.f32 ? launch_wavespeed<float>(&view, base, sim->gamma, acc, fin, st)
+                   : launch_wavespeed<double>(&view, base, sim->gamma, acc, fin, st);
   if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
   return kOk;
 }
@@ -444,10 +478,14 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res, double s
 int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
   if (sim == nullptr || sim->a == nullptr) return fail(kEInval, "fl_sim_begin not called");
   if (nsteps < 0) return fail(kEInval, "nsteps < 0");
+  if (sim->external) return fail(kEInval, "external reduction: step with fl_sim_sweep");
+  if (sim->cursor != 0) return fail(kEInval, "a step is half done (fl_sim_sweep)");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int D = sim->grid.dims;
   SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, 0.0, sim->boundary);
   p.ctrl = sim->ctrl;
+  p.ws_lo = sim->own_lo;
+  p.ws_hi = sim->own_hi;
   for (int64_t k = 0; k < nsteps; ++k) {
     // input of this step: for even D the state returns to buffer a every
     // step; for odd D it alternates a, b, a, ...
@@ -470,6 +508,72 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
     }
     sim->enqueued += 1;
   }
+  return kOk;
+}
+
+int fl_sim_set_rows(fl_sim* sim, int64_t row_lo, int64_t row_hi) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  const int64_t n = sim->grid.n[sim->grid.dims - 1];
+  if (!(row_lo == 0 && row_hi == 0) && !(0 <= row_lo && row_lo < row_hi && row_hi <= n))
+    return fail(kEInval, "rows [%lld, %lld) outside [0, %lld)", (long long)row_lo,
+                (long long)row_hi, (long long)n);
+  sim->own_lo = row_lo;
+  sim->own_hi = row_hi;
+  return kOk;
+}
+
+int fl_sim_set_external_reduce(fl_sim* sim, int on) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  sim->external = on ? 1 : 0;
+  return kOk;
+}
+
+int fl_sim_set_ws_word(fl_sim* sim, void* word) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  if (word != nullptr && (reinterpret_cast<uintptr_t>(word) & 7u))
+    return fail(kEInval, "the wavespeed word must be 8-byte aligned");
+  sim->ws_word = static_cast<unsigned long long*>(word);
+  return kOk;
+}
+
+int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
+  if (sim == nullptr || sim->a == nullptr) return fail(kEInval, "fl_sim_begin not called");
+  const int D = sim->grid.dims;
+  if (dim != sim->cursor) return fail(kEInval, "sweep %d expected, %d given", sim->cursor, dim);
+  const bool from_b = (D % 2 == 1) && ((sim->enqueued & 1) == 1);
+  void* si = from_b ? sim->b : sim->a;
+  void* so = from_b ? sim->a : sim->b;
+  if (D != 1 && (dim & 1)) {  // sweeps alternate direction between the buffers
+    void* t = si;
+    si = so;
+    so = t;
+  }
+  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, 0.0, sim->boundary);
+  p.ctrl = sim->ctrl;
+  p.ws_lo = sim->own_lo;
+  p.ws_hi = sim->own_hi;
+  p.in = si;
+  p.out = so;
+  const bool last = (dim == D - 1);
+  p.ws_accum = last ? (sim->external ? sim->ws_word : &sim->ctrl->ws_bits) : nullptr;
+  p.finalize = (last && !sim->external) ? 1 : 0;
+  cudaError_t e = launch_sweep(p, sim->pol, D, dim, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_sweep");
+  if (last) {
+    sim->cursor = 0;
+    sim->enqueued += 1;
+  } else {
+    sim->cursor = dim + 1;
+  }
+  return kOk;
+}
+
+int fl_sim_finalize(fl_sim* sim, int advance, void* stream) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  finalize_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      sim->ctrl, sim->external ? sim->ws_word : nullptr, advance);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_finalize");
   return kOk;
 }
 

@@ -323,6 +323,8 @@ __global__ void __launch_bounds__(WalkCfg<T, S>::THREADS) batch2d_kernel(BatchAr
   p.reflect = a.reflect;
   p.ctrl = nullptr;
   p.ws_accum = nullptr;
+  p.ws_lo = 0;
+  p.ws_hi = 0;
   p.finalize = 0;
   const int warp = threadIdx.x >> 5;
   const int64_t y0 = ((int64_t)it.by * W::WARPS + warp) * pr.ry;

@@ -43,7 +43,15 @@ struct SweepParams {
   StepControl* ctrl;      // nullable: take dtdh / done from the control block
   unsigned long long* ws_accum;  // nullable: max wavespeed of the output (double bits)
   int finalize;           // 1: last sweep of a step; the last block advances ctrl
+  // rows (index along the slowest dimension) whose cells enter the fused
+  // max wavespeed: [ws_lo, ws_hi); every row when ws_hi <= ws_lo.  A slab
+  // of a decomposed grid counts its own rows, not its ghost rows.
+  int64_t ws_lo, ws_hi;
 };
+
+__host__ __device__ __forceinline__ bool ws_row_counts(const SweepParams& p, int64_t row) {
+  return p.ws_hi <= p.ws_lo || (row >= p.ws_lo && row < p.ws_hi);
+}
 
 // Status codes, mirrored by include/fluidity_b200.h.
 enum : int {

@@ -341,7 +341,8 @@ sweep_kernel(SweepParams p) {
       r.v[c] = sU[c * G::R + q] + dtdh * (sFX[c * G::F + fi] - sFX[c * G::F + fi + FS]);
 #pragma unroll
     for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-    if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+    if (want_ws && ws_row_counts(p, D == 1 ? g0 : (D == 2 ? g1 : g2)))
+      ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
   }
   if (want_ws)
     cta_wavespeed_commit<NT>(ws_local, p.ws_accum, p.ctrl, p.finalize, true, s_red);

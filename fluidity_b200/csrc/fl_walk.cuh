@@ -213,7 +213,8 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
           const int64_t gi = j * n0 + x;
 #pragma unroll
           for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-          if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+          if (want_ws && ws_row_counts(p, j))
+            ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
         }
       } else {
         if (j >= y0) {
@@ -229,7 +230,8 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
             const int64_t gi = (j - 1) * n0 + x;
 #pragma unroll
             for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-            if (want_ws) ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+            if (want_ws && ws_row_counts(p, j - 1))
+              ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
           }
           f_prev = fxy;
         }

@@ -138,6 +138,34 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res,
  * launched but do no work. */
 int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream);
 
+/* ---- one slab of a grid decomposed across GPUs (no reference counterpart:
+ * the reference runs one GPU).  A rank holds its own rows (along the slowest
+ * dimension) plus ghost rows that the host refreshes from the neighbouring
+ * ranks before every sweep; the CFL maximum is reduced across ranks by the
+ * host between the last sweep of a step and fl_sim_finalize. */
+
+/* Rows [row_lo, row_hi) of the slowest dimension are this rank's own; only
+ * their cells enter the wavespeed maxima (both 0: every row).  Set before
+ * fl_sim_begin. */
+int fl_sim_set_rows(fl_sim* sim, int64_t row_lo, int64_t row_hi);
+
+/* on != 0: fl_sim_begin (which zeroes it) and the last sweep of each step
+ * only accumulate the max wavespeed, as the bits of a non-negative double,
+ * into the caller's 8-byte device word given to fl_sim_set_ws_word; the host
+ * reduces that word over ranks (64-bit integer MAX) and then calls
+ * fl_sim_finalize, which consumes and clears it. */
+int fl_sim_set_external_reduce(fl_sim* sim, int on);
+int fl_sim_set_ws_word(fl_sim* sim, void* word);
+
+/* Enqueues sweep `dim` of the current step (dims in order 0, 1, ...), so
+ * that the host can exchange ghost rows between sweeps. */
+int fl_sim_sweep(fl_sim* sim, int dim, void* stream);
+
+/* From the (reduced) wavespeed word: the next dt and dtdh and, with
+ * advance != 0, run_time += dt, iters += 1 and the stop test -- the
+ * finalisation the fused reduction otherwise does in its last block. */
+int fl_sim_finalize(fl_sim* sim, int advance, void* stream);
+
 /* Waits for the stream and reports the loop state.  *result points at the
  * buffer (a or b) holding the latest state.  Returns FL_ENAN if a wavespeed
  * was not finite. */
