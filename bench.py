@@ -565,6 +565,19 @@ def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
             res.update({"fd_directions": directions,
                         "fd_eps_1e-6": _fd_summary(e6), "fd_eps_1e-7": _fd_summary(e7),
                         "fd_max_rel_err": max(e6)})
+            # the same check without the flattening coefficient, which the
+            # adjoint holds frozen: there the adjoint is the exact derivative
+            # away from limiter and wave-speed switches
+            adj_nf = Adjoint((n, n), steps, dtype=dtype, flatten=False)
+            rho_nf = rho0.detach().clone().requires_grad_(True)
+            with torch.no_grad():
+                pt_nf = pressure(adj_nf.forward(state_from_density(
+                    gaussian_density(n, 2, dtype=tdt)), 0.7))
+            objective(rollout(state_from_density(rho_nf), adj_nf, 0.7), pt_nf).backward()
+            enf = _fd_check(adj_nf, rho_nf.detach(), rho_nf.grad.detach(), pt_nf, directions,
+                            eps)
+            res["fd_no_flattening_eps_1e-6"] = _fd_summary(enf)
+            del adj_nf
         else:
             g64 = grads["f64"]
             res["rel_diff_vs_f64_gradient"] = (torch.norm(grads["f32"] - g64) /

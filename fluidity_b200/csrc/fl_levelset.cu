@@ -17,9 +17,10 @@
 //    seeds the signed value), every other cell
 //    relaxes to the fixed point of the Godunov local eikonal solve
 //    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles relax in shared
-//    memory and in place, only tiles stamped by a changed neighbour run the
-//    next pass, and the host checks convergence once per 16 passes; the
-//    result takes the input's sign (set_signs, :96-112).
+//    memory, passes ping-pong between two buffers, only tiles stamped by a
+//    changed neighbour relax in the next pass (the others copy), and the
+//    host checks convergence once per 16 passes; the result takes the
+//    input's sign (set_signs, :96-112).
 // FP64 level sets on 2-D grids; out-of-domain reads mirror the domain.
 #include <cuda_runtime.h>
 
@@ -193,37 +194,36 @@ __device__ __forceinline__ double eik_local(double xm, double xp, double ym, dou
   return 0.5 * (a + b + sqrt(2.0 * fh * fh - (amb * amb)));
 }
 
-// Pass k over the tiles, in place on d.  A tile runs in pass 0 and in every
-// pass whose number its stamp has reached (a changed tile stamps itself and
-// its eight neighbours with k + 1).  It loads itself and a one-cell halo (+max
-// outside the domain), relaxes FIM_INNER rounds in shared memory and writes
-// back.  Neighbouring tiles may update their cells while this tile reads its
-// halo; every value read is then either the old or the new one, both upper
-// bounds of the fixed point, and since each update only lowers a value
-// through a monotone local solve, the relaxation reaches the same fixed point
-// whatever the interleaving.  A pass after one that changed nothing returns
-// at once (last_change < k - 1).
+// Pass k over the tiles: reads src (the previous pass) and writes dst.  A
+// tile runs in pass 0 and in every pass whose number its stamp has reached (a
+// changed tile stamps itself and its eight neighbours with k + 1); it loads
+// itself and a one-cell halo (+max outside the domain), relaxes FIM_INNER
+// rounds in shared memory and writes its cells to dst.  A tile that does not
+// run copies its cells from src to dst.  Every pass therefore depends only on
+// the previous one and the result is deterministic.  A pass after one that
+// changed nothing returns at once (last_change < k - 1) without writing.
 __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
-    double* __restrict__ d, const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny,
-    double h, int* __restrict__ stamp, int tiles_x, int tiles_y, int* __restrict__ last_change,
-    int k) {
+    const double* __restrict__ src, double* __restrict__ dst,
+    const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny, double h,
+    int* __restrict__ stamp, int tiles_x, int tiles_y, int* __restrict__ last_change, int k) {
   if (k > 0 && *(volatile int*)last_change < k - 1) return;
   const int t = blockIdx.x;
-  if (k > 0 && *(volatile int*)(stamp + t) < k) return;
   const int tx0 = t % tiles_x, ty0 = t / tiles_x;
   const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
   const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
   const bool in = x < nx && y < ny;
   const int64_t i = y * nx + x;
+  if (k > 0 && stamp[t] < k) {
+    if (in) dst[i] = src[i];
+    return;
+  }
   __shared__ double s[FT + 2][FT + 2];
   __shared__ int changed;
   if (threadIdx.x == 0) changed = 0;
   for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
     const int hx = q % (FT + 2), hy = q / (FT + 2);
     const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
-    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
-                    ? *(volatile const double*)(d + gy * nx + gx)
-                    : DBL_MAX;
+    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
   }
   __syncthreads();
   const bool free_cell = in && !fixed[i];
@@ -239,10 +239,8 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     }
     __syncthreads();
   }
-  if (mine) {
-    d[i] = s[ly + 1][lx + 1];
-    changed = 1;
-  }
+  if (in) dst[i] = s[ly + 1][lx + 1];
+  if (mine) changed = 1;
   __syncthreads();
   if (threadIdx.x == 0 && changed) {
     atomicMax(last_change, k);
@@ -288,9 +286,9 @@ int64_t fl_ls_workspace_bytes(const fl_grid* grid) {
   if (check_ls_grid(grid) != kOk) return -1;
   const int64_t n = grid->n[0] * grid->n[1];
   const int64_t tiles = ((grid->n[0] + FT - 1) / FT) * ((grid->n[1] + FT - 1) / FT);
-  // two FP64 planes (RK3 stages), fixed-cell flags of the reinitialisation,
-  // its tile stamps (room for two ints per tile) and its change counter,
-  // each 256-byte aligned
+  // two FP64 planes (RK3 stages; the first also the reinitialisation's
+  // second buffer), its fixed-cell flags, tile stamps (room for two ints per
+  // tile) and change counter, each 256-byte aligned
   auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
   return al(2 * n * 8) + al(n) + al(2 * tiles * 4) + 256;
 }
@@ -367,7 +365,9 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
   unsigned char* fixed = reinterpret_cast<unsigned char*>(w + al(2 * n * 8));
   int* stamp = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n));
   int* last = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(2 * tiles * 4));
-  // the relaxation runs in place in `out`
+  // passes ping-pong between `out` (even passes read it) and the first
+  // workspace plane
+  double* buf[2] = {out, reinterpret_cast<double*>(w)};
   fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, out, fixed);
   fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(stamp, tiles, 0);
   fill_int_kernel<<<1, 32, 0, st>>>(last, 1, 0);
@@ -380,8 +380,8 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
   while (e == cudaSuccess && !converged && launched < max_passes) {
     const int end = launched + CHUNK < max_passes ? launched + CHUNK : max_passes;
     for (int k = launched; k < end; ++k)
-      fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(out, fixed, nx, ny, h, stamp, tiles_x, tiles_y,
-                                                 last, k);
+      fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(buf[k & 1], buf[(k + 1) & 1], fixed, nx, ny, h,
+                                                 stamp, tiles_x, tiles_y, last, k);
     launched = end;
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h_last, last, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -389,6 +389,12 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
     // converged once a pass after the last change has run
     converged = (e == cudaSuccess) && (h_last + 1 < launched);
   }
+  // the last pass that ran (h_last + 1, which changed nothing) wrote
+  // buf[(h_last + 2) & 1]
+  if (e == cudaSuccess && converged && ((h_last + 2) & 1))
+    e = cudaMemcpyAsync(out, buf[1], n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && !converged && (launched & 1))
+    e = cudaMemcpyAsync(out, buf[1], n * sizeof(double), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) {
     fim_sign_kernel<<<grid1d(n), 256, 0, st>>>(phi, out, n);
     e = cudaGetLastError();

@@ -208,6 +208,24 @@ def test_reinit_matches_oracle(cuda, oracle, nx, ny, seed, scale):
 
 
 @pytest.mark.gpu
+def test_reinit_is_deterministic_and_odd(cuda):
+    """Repeated calls give identical results, and reinit(-phi) = -reinit(phi)
+    bit for bit (the two-material path relies on it: its level sets are
+    reinitialised separately and must stay negatives of each other)."""
+    import torch
+    nx, ny = 300, 170
+    phi, h = circle_phi(nx, ny, 6)
+    phi = phi * 1.3
+    ops = _ops((nx, ny))
+    t = torch.tensor(phi, device=cuda)
+    a = ops.reinit(t, h).cpu().numpy()
+    for _ in range(3):
+        assert np.array_equal(ops.reinit(t, h).cpu().numpy(), a)
+    b = ops.reinit(-t, h).cpu().numpy()
+    assert np.array_equal(b, -a)
+
+
+@pytest.mark.gpu
 def test_reinit_pass_limit_reports_timeout(cuda):
     import torch
     from fluidity_b200 import capi
