@@ -162,8 +162,14 @@ __global__ void ls_project_kernel(int64_t n, double* a, double* b) {
 
 // ---- reinitialisation ------------------------------------------------------
 
-constexpr int FT = 16;                 // tile side
-constexpr int FIM_INNER = 24;          // in-tile relaxation rounds per pass
+#ifndef FL_FIM_TILE
+#define FL_FIM_TILE 16
+#endif
+#ifndef FL_FIM_PERSIST
+#define FL_FIM_PERSIST 1
+#endif
+constexpr int FT = FL_FIM_TILE;              // tile side
+constexpr int FIM_INNER = 3 * FL_FIM_TILE / 2;  // in-tile relaxation rounds per pass
 
 __device__ __forceinline__ int dsgn(double v) { return (0.0 < v) - (v < 0.0); }
 
@@ -195,60 +201,81 @@ __device__ __forceinline__ double eik_local(double xm, double xp, double ym, dou
 }
 
 // Pass k over the tiles: reads src (the previous pass) and writes dst.  A
-// tile runs in pass 0 and in every pass whose number its stamp has reached (a
-// changed tile stamps itself and its eight neighbours with k + 1); it loads
-// itself and a one-cell halo (+max outside the domain), relaxes FIM_INNER
-// rounds in shared memory and writes its cells to dst.  A tile that does not
-// run copies its cells from src to dst.  Every pass therefore depends only on
-// the previous one and the result is deterministic.  A pass after one that
-// changed nothing returns at once (last_change < k - 1) without writing.
+// tile relaxes in pass 0 and in every pass whose number its stamp has
+// reached (a changed tile stamps itself and its eight neighbours with k + 1);
+// it loads itself and a one-cell halo (+max outside the domain), relaxes
+// FIM_INNER rounds in shared memory and writes its cells to dst.  A tile that
+// does not relax must hand its values on to dst; it copies them unless both
+// buffers already hold them (synced[t]: set when a tile copies or relaxes
+// without change, cleared when it changes).  Every pass depends only on the
+// previous one, so the result is deterministic.  CTAs loop over the tiles.
+// A pass after one that changed nothing returns at once (last_change < k - 1)
+// without writing.
 __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     const double* __restrict__ src, double* __restrict__ dst,
     const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny, double h,
-    int* __restrict__ stamp, int tiles_x, int tiles_y, int* __restrict__ last_change, int k) {
+    int* __restrict__ stamp, int* __restrict__ synced, int tiles_x, int tiles_y,
+    int* __restrict__ last_change, int k) {
   if (k > 0 && *(volatile int*)last_change < k - 1) return;
-  const int t = blockIdx.x;
-  const int tx0 = t % tiles_x, ty0 = t / tiles_x;
-  const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
-  const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
-  const bool in = x < nx && y < ny;
-  const int64_t i = y * nx + x;
-  if (k > 0 && stamp[t] < k) {
-    if (in) dst[i] = src[i];
-    return;
-  }
   __shared__ double s[FT + 2][FT + 2];
   __shared__ int changed;
-  if (threadIdx.x == 0) changed = 0;
-  for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
-    const int hx = q % (FT + 2), hy = q / (FT + 2);
-    const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
-    s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
-  }
-  __syncthreads();
-  const bool free_cell = in && !fixed[i];
-  bool mine = false;
-  for (int r = 0; r < FIM_INNER; ++r) {
-    double q = 0.0;
-    if (free_cell)
-      q = eik_local(s[ly + 1][lx], s[ly + 1][lx + 2], s[ly][lx + 1], s[ly + 2][lx + 1], h);
-    __syncthreads();
-    if (free_cell && q < s[ly + 1][lx + 1]) {
-      s[ly + 1][lx + 1] = q;
-      mine = true;
+  __shared__ int mode;   // 0: relax, 1: copy, 2: nothing to do
+  const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
+  const int tiles = tiles_x * tiles_y;
+  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int tx0 = t % tiles_x, ty0 = t / tiles_x;
+    const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
+    const bool in = x < nx && y < ny;
+    const int64_t i = y * nx + x;
+    // a neighbour may raise stamp[t] during this pass: one thread reads it
+    // and the whole CTA follows that reading
+    if (threadIdx.x == 0) {
+      const int st = *(volatile int*)(stamp + t);
+      mode = (k == 0 || st >= k) ? 0 : (synced[t] ? 2 : 1);
+      changed = 0;
     }
     __syncthreads();
-  }
-  if (in) dst[i] = s[ly + 1][lx + 1];
-  if (mine) changed = 1;
-  __syncthreads();
-  if (threadIdx.x == 0 && changed) {
-    atomicMax(last_change, k);
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int ax = tx0 + dx, ay = ty0 + dy;
-        if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y) stamp[ay * tiles_x + ax] = k + 1;
+    if (mode != 0) {
+      if (mode == 1 && in) dst[i] = src[i];
+      if (mode == 1 && threadIdx.x == 0) synced[t] = 1;
+      __syncthreads();   // mode is rewritten for the next tile
+      continue;
+    }
+    for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
+      const int hx = q % (FT + 2), hy = q / (FT + 2);
+      const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
+      s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
+    }
+    __syncthreads();
+    const bool free_cell = in && !fixed[i];
+    bool mine = false;
+    for (int r = 0; r < FIM_INNER; ++r) {
+      double q = 0.0;
+      if (free_cell)
+        q = eik_local(s[ly + 1][lx], s[ly + 1][lx + 2], s[ly][lx + 1], s[ly + 2][lx + 1], h);
+      __syncthreads();
+      if (free_cell && q < s[ly + 1][lx + 1]) {
+        s[ly + 1][lx + 1] = q;
+        mine = true;
       }
+      __syncthreads();
+    }
+    if (in) dst[i] = s[ly + 1][lx + 1];
+    if (mine) changed = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      synced[t] = changed ? 0 : 1;
+      if (changed) {
+        atomicMax(last_change, k);
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int ax = tx0 + dx, ay = ty0 + dy;
+            if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y)
+              stamp[ay * tiles_x + ax] = k + 1;
+          }
+      }
+    }
+    __syncthreads();   // s and changed are reused by the next tile
   }
 }
 
@@ -369,19 +396,25 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
   // workspace plane
   double* buf[2] = {out, reinterpret_cast<double*>(w)};
   fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, out, fixed);
-  fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(stamp, tiles, 0);
+  fill_int_kernel<<<grid1d(2 * tiles), 256, 0, st>>>(stamp, 2 * tiles, 0);  // stamps, synced
   fill_int_kernel<<<1, 32, 0, st>>>(last, 1, 0);
   // passes are launched in chunks; the host reads the last pass that changed
   // anything after each chunk (passes past convergence return at once)
   constexpr int CHUNK = 16;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = 2048 / (FT * FT);
+  const int pass_ctas = (FL_FIM_PERSIST && tiles > sms * per_sm) ? sms * per_sm : tiles;
   int launched = 0, h_last = 0;
   bool converged = false;
   cudaError_t e = cudaGetLastError();
   while (e == cudaSuccess && !converged && launched < max_passes) {
     const int end = launched + CHUNK < max_passes ? launched + CHUNK : max_passes;
     for (int k = launched; k < end; ++k)
-      fim_pass_kernel<<<tiles, FT * FT, 0, st>>>(buf[k & 1], buf[(k + 1) & 1], fixed, nx, ny, h,
-                                                 stamp, tiles_x, tiles_y, last, k);
+      fim_pass_kernel<<<pass_ctas, FT * FT, 0, st>>>(buf[k & 1], buf[(k + 1) & 1], fixed, nx, ny,
+                                                     h, stamp, stamp + tiles, tiles_x, tiles_y,
+                                                     last, k);
     launched = end;
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h_last, last, sizeof(int), cudaMemcpyDeviceToHost, st);
