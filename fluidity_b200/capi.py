@@ -77,6 +77,10 @@ _G = C.POINTER(Grid)
 PROTOTYPES = {
     "fl_version": (C.c_int, []),
     "fl_last_error_string": (C.c_char_p, []),
+    "fl_policy_from_settings": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),
+                                          C.POINTER(C.c_int32)]),
+    "fl_policy_from_settings_file": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),
+                                               C.POINTER(C.c_int32)]),
     "fl_state_bytes": (C.c_int64, [_G, C.c_uint32]),
     "fl_split_sweep": (C.c_int, [_G, C.c_int, _P, _P, C.c_double, C.c_double, C.c_uint32,
                                  C.c_uint32, _P, _P]),
@@ -173,3 +177,12 @@ def check(rc: int, lib=None) -> None:
         lib = lib or load()
         msg = lib.fl_last_error_string().decode(errors="replace")
         raise FlError(rc, msg)
+
+
+def policy_from_settings(text: str):
+    """(policy bits, dims) from a fluidity settings text's simulator block."""
+    lib = load()
+    pol = C.c_uint32()
+    dims = C.c_int32()
+    check(lib.fl_policy_from_settings(text.encode(), C.byref(pol), C.byref(dims)), lib)
+    return int(pol.value), int(dims.value)

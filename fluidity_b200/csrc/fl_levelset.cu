@@ -169,7 +169,10 @@ __global__ void ls_project_kernel(int64_t n, double* a, double* b) {
 #define FL_FIM_PERSIST 1
 #endif
 constexpr int FT = FL_FIM_TILE;              // tile side
-constexpr int FIM_INNER = 3 * FL_FIM_TILE / 2;  // in-tile relaxation rounds per pass
+#ifndef FL_FIM_INNER
+#define FL_FIM_INNER (3 * FL_FIM_TILE / 2)
+#endif
+constexpr int FIM_INNER = FL_FIM_INNER;  // in-tile relaxation rounds per pass
 
 __device__ __forceinline__ int dsgn(double v) { return (0.0 < v) - (v < 0.0); }
 

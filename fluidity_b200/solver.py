@@ -156,6 +156,44 @@ class Simulation:
         return self._bufs[out.value], int(it.value), float(rt.value)
 
 
+def write_separate_raw(u, shape, gamma, prefix, sim_time):
+    """write_results_separate_raw (simulator/simulator_impl.hpp:360-420) for a
+    host state u ((dims + 2, >= cells) conservative planes): one file per
+    primitive variable, <prefix>_<name>_<sim_time>.dat, values formatted as a
+    C++ stream's default (%g) each followed by a space; 1-D: one line then a
+    blank line; 2-D: one line per row; 3-D: the 2-D files of plane z under
+    <prefix>_<z>.  Primitives are computed in the state's precision."""
+    u = np.asarray(u)
+    D = len(shape)
+    cells = int(np.prod(shape))
+    T = u.dtype.type
+    rho = u[0, :cells]
+    v = [u[2 + d, :cells] / rho for d in range(D)]
+    v2 = T(0)
+    for d in range(D):
+        v2 = v2 + v[d] * v[d]
+    p = (T(gamma) - T(1)) * (u[1, :cells] - T(0.5) * rho * v2)
+    prim = [rho, p] + v
+    names = ["rho", "p", "v_x", "v_y", "v_z"][:D + 2]
+    nx = shape[0]
+    ny = shape[1] if D >= 2 else 1
+    nz = shape[2] if D == 3 else 1
+    stamp = f"{float(sim_time):f}"
+    paths = []
+    for z in range(nz):
+        pre = f"{prefix}_{z}" if D == 3 else prefix
+        for k, name in enumerate(names):
+            path = f"{pre}_{name}_{stamp}.dat"
+            plane = prim[k].reshape(nz, ny, nx)[z]
+            with open(path, "w") as f:
+                for y in range(ny):
+                    f.write("".join("%g " % float(val) for val in plane[y]) + "\n")
+                if D == 1:
+                    f.write("\n")
+            paths.append(path)
+    return paths
+
+
 class SimulatorImpl:
     """sim::SimulatorImpl (simulator/simulator_impl.hpp:43-512) on one B200.
 
@@ -215,6 +253,25 @@ class SimulatorImpl:
 
     def states(self) -> np.ndarray:
         return self.state.double().cpu().numpy()
+
+    def write_results_separate_raw(self, prefix: str):
+        """One file per primitive variable (simulator_impl.hpp:413-420)."""
+        return write_separate_raw(self.states(), self.shape(), self.kw["gamma"], prefix,
+                                  self.sim_time)
+
+    @classmethod
+    def from_settings(cls, text: str, gamma: float = 1.4, boundary_mask: int = 0):
+        """A simulator configured by a fluidity settings text's
+        "simulator : { ... }" block (setting/simulator_parameter.hpp), the
+        run-time form of OptionManager::create (setting/option_manager.hpp
+        :241-246)."""
+        pol, dims = capi.policy_from_settings(text)
+        sim = cls(dims=dims, gamma=gamma, boundary_mask=boundary_mask)
+        sim.kw["dtype"] = "f32" if pol & 1 else "f64"
+        sim.kw["flux"] = {0: "hllc", 1: "force", 2: "lf", 3: "richtmyer"}[(pol >> 1) & 3]
+        sim.kw["limiter"] = "superbee" if (pol >> 3) & 1 else "vanleer"
+        sim.kw["recon"] = "basic" if (pol >> 4) & 1 else "muscl"
+        return sim
 
     def write_results(self, prefix: str):
         """ASCII columns: position(s) then rho, p, v... (primitive), one cell per

@@ -63,6 +63,20 @@ typedef struct fl_grid {
   int64_t pitch;
 } fl_grid;
 
+/* Settings-file dispatch: the "simulator : { data_type : ..., dimensions : ...,
+ * limit_form : ..., limiter : ..., material : ..., reconstructor : ...,
+ * flux_method : ..., solve_method : ..., execution : ... }" block of a
+ * fluidity settings text (Settings::from_string, setting/settings.hpp:50-105;
+ * SimulatorParameter, setting/simulator_parameter.hpp:29-105) turned into the
+ * policy bits and dimension count that OptionManager::create
+ * (setting/option_manager.hpp:241-246) would have turned into a SimulatorImpl
+ * type.  Missing entries take SimTraits' defaults (double, one, ideal-gas,
+ * conservative, superbee, muscl-hancock, force, split, gpu); choices this
+ * library does not build (primitive limit form, void/linear limiters,
+ * unsplit) return FL_EINVAL.  Host-only: no device is touched. */
+int fl_policy_from_settings(const char* text, uint32_t* policy, int32_t* dims);
+int fl_policy_from_settings_file(const char* path, uint32_t* policy, int32_t* dims);
+
 /* Library version (major * 10000 + minor * 100 + patch). */
 int fl_version(void);
 

@@ -380,6 +380,45 @@ class SimulatorImpl {
     }
   }
 
+  // write_results_separate_raw (simulator_impl.hpp:360-420): one file per
+  // primitive variable, <prefix>_<name>_<sim_time>.dat with the stream's
+  // default formatting; 1-D: the values on one line then a blank line;
+  // 2-D: one line per row of x values; 3-D: the 2-D files of each z plane
+  // under <prefix>_<z>.
+  void write_results_separate_raw(const std::string& prefix) const {
+    const fl_grid g = grid();
+    const auto h = result_->as_host();
+    const T gm = mat_.adiabatic();
+    const char* names[5] = {"rho", "p", "v_x", "v_y", "v_z"};
+    const int nz = dimensions == 3 ? (int)g.n[2] : 1;
+    for (int z = 0; z < nz; ++z) {
+      const std::string pre = dimensions == 3 ? prefix + "_" + std::to_string(z) : prefix;
+      std::vector<std::ofstream> streams;
+      for (std::size_t k = 0; k < dimensions + 2; ++k)
+        streams.emplace_back(pre + "_" + names[k] + "_" + std::to_string(sim_time_) + ".dat");
+      const int64_t ny = dimensions >= 2 ? g.n[1] : 1;
+      for (int64_t y = 0; y < ny; ++y) {
+        for (int64_t x = 0; x < g.n[0]; ++x) {
+          const int64_t i = ((int64_t)z * g.n[1] + y) * g.n[0] + x;
+          const T rho = h[i];
+          T v2 = 0;
+          T v[3] = {0, 0, 0};
+          for (std::size_t d = 0; d < dimensions; ++d) {
+            v[d] = h[(2 + d) * g.pitch + i] / rho;
+            v2 += v[d] * v[d];
+          }
+          const T p = (gm - T(1)) * (h[g.pitch + i] - T(0.5) * rho * v2);
+          streams[0] << rho << " ";
+          streams[1] << p << " ";
+          for (std::size_t d = 0; d < dimensions; ++d) streams[2 + d] << v[d] << " ";
+        }
+        for (auto& st : streams) st << "\n";
+      }
+      if (dimensions == 1)
+        for (auto& st : streams) st << "\n";
+    }
+  }
+
  private:
   Material mat_{};
   solver::BoundarySetter setter_{};

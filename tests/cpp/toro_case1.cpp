@@ -1,8 +1,10 @@
 // Toro's test 1 (Sod-like shock tube) through the C++ policy interface, set up
 // the way the reference's validation/1d_toro_case_1_validation.cu does:
 // resolution 0.0025 on [0, 1], membrane at 0.3, sim_time 0.2, CFL 0.9.
-// Writes the final primitive state to argv[1].dat.
+// Writes the final primitive state to argv[1].dat and, one file per
+// variable, to argv[1]_raw_<name>_0.200000.dat.
 #include <cstdio>
+#include <string>
 
 #include "fluidity_b200/fluidity.hpp"
 
@@ -31,6 +33,7 @@ int main(int argc, char** argv) {
     });
     simulator.simulate();
     simulator.write_results(argv[1]);
+    simulator.write_results_separate_raw(std::string(argv[1]) + "_raw");
     std::printf("iterations %lld run_time %.17g\n", (long long)simulator.iterations(),
                 simulator.run_time());
   } catch (const fluid::Error& e) {

@@ -45,3 +45,9 @@ def test_cpp_toro_case1_matches_oracle(cuda, oracle, tmp_path):
     rp = oracle.cons_to_prim(ref, 1.4)
     got = data[:, 1:].T                    # rho, p, v_x
     assert np.max(np.abs(got - rp) / np.maximum(np.abs(rp), 1e-3)) < 1e-9
+    for k, name in enumerate(["rho", "p", "v_x"]):
+        text = open(str(tmp_path / f"toro1_raw_{name}_0.200000.dat")).read()
+        assert text.endswith(" \n\n")
+        vals = np.array([float(t) for t in text.split()])
+        assert vals.shape == (n,)
+        assert np.allclose(vals, rp[k], rtol=1e-5, atol=1e-6)
