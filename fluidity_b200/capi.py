@@ -66,6 +66,11 @@ def policy_bits(dtype: str = "f64", flux: str = "hllc", limiter: str = "vanleer"
     return bits
 
 
+class Material(C.Structure):
+    """fl_material: the ideal gas (p_inf = 0) or the stiffened fluid."""
+    _fields_ = [("gamma", C.c_double), ("p_inf", C.c_double)]
+
+
 class BatchDesc(C.Structure):
     _fields_ = [("dims", C.c_int32), ("n", C.c_int64 * 2), ("offset", C.c_int64),
                 ("pitch", C.c_int64), ("res", C.c_double)]
@@ -82,6 +87,16 @@ PROTOTYPES = {
     "fl_policy_from_settings_file": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),
                                                C.POINTER(C.c_int32)]),
     "fl_state_bytes": (C.c_int64, [_G, C.c_uint32]),
+    "fl_split_sweep_mat": (C.c_int, [_G, C.c_int, _P, _P, C.POINTER(Material), C.c_double,
+                                     C.c_uint32, C.c_uint32, _P, _P]),
+    "fl_split_solve_mat": (C.c_int, [_G, C.POINTER(_P), C.POINTER(_P), C.POINTER(Material),
+                                     C.c_double, C.c_uint32, C.c_uint32, _P, _P]),
+    "fl_max_wavespeed_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
+    "fl_fill_riemann_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
+    "fl_sim_set_material": (C.c_int, [_P, C.POINTER(Material)]),
+    "fl_mm_set_materials": (C.c_int, [_P, C.POINTER(Material)]),
+    "fl_mm_set_states_mat": (C.c_int, [_G, C.c_uint32, _P, _P, C.POINTER(C.c_double),
+                                       C.POINTER(Material), _P]),
     "fl_split_sweep": (C.c_int, [_G, C.c_int, _P, _P, C.c_double, C.c_double, C.c_uint32,
                                  C.c_uint32, _P, _P]),
     "fl_split_solve": (C.c_int, [_G, C.POINTER(_P), C.POINTER(_P), C.c_double, C.c_double,

@@ -87,15 +87,23 @@ int check_policy(uint32_t policy) {
   return kOk;
 }
 
+int check_material(const fl_material* m) {
+  if (m == nullptr) return fail(kEInval, "material is NULL");
+  if (!(m->gamma > 1.0)) return fail(kEInval, "gamma must exceed 1");
+  if (!(m->p_inf >= 0.0) || m->p_inf > DBL_MAX) return fail(kEInval, "p_inf must be finite and >= 0");
+  return kOk;
+}
+
 size_t elem_size(const Policy& p) { return p.f32 ? sizeof(float) : sizeof(double); }
 
-SweepParams make_params(const fl_grid* g, const Policy& pol, double gamma, double dtdh,
-                        uint32_t boundary) {
+SweepParams make_params(const fl_grid* g, const Policy& pol, double gamma, double pinf,
+                        double dtdh, uint32_t boundary) {
   SweepParams p;
   memset(&p, 0, sizeof(p));
   p.pitch = g->pitch;
   for (int d = 0; d < 3; ++d) p.n[d] = g->n[d];
   p.gamma = gamma;
+  p.pinf = pinf;
   p.dtdh = dtdh;
   p.limiter = pol.limiter;
   p.basic = pol.basic;
@@ -114,7 +122,7 @@ cudaError_t launch_sweep(const SweepParams& p, const Policy& pol, int dims, int 
 
 template <typename T, int D>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const T* __restrict__ in, int64_t pitch,
-                                                        int64_t cells, T gamma,
+                                                        int64_t cells, T gamma, T pinf,
                                                         unsigned long long* accum,
                                                         StepControl* ctrl) {
   __shared__ double s_red[8];
@@ -124,13 +132,14 @@ __global__ void __launch_bounds__(256) wavespeed_kernel(const T* __restrict__ in
     Cons<T, D> u;
 #pragma unroll
     for (int c = 0; c < D + 2; ++c) u.v[c] = __ldg(in + c * pitch + i);
-    ws_max(local, (double)max_wavespeed(u, gamma));
+    // p + p_inf under the root; p_inf = 0 leaves the ideal gas's value
+    ws_max(local, (double)max_wavespeed<true>(u, gamma, pinf));
   }
   cta_wavespeed_commit<256>(local, accum, ctrl, ctrl != nullptr ? 1 : 0, false, s_red);
 }
 
 template <typename T>
-cudaError_t launch_wavespeed(const fl_grid* g, const void* in, double gamma,
+cudaError_t launch_wavespeed(const fl_grid* g, const void* in, double gamma, double pinf,
                              unsigned long long* accum, StepControl* ctrl, cudaStream_t st) {
   const int64_t cells = g->n[0] * g->n[1] * g->n[2];
   int dev = 0, sms = 148;
@@ -141,9 +150,9 @@ cudaError_t launch_wavespeed(const fl_grid* g, const void* in, double gamma,
   if (blocks < 1) blocks = 1;
   const T* p = static_cast<const T*>(in);
   switch (g->dims) {
-    case 1: wavespeed_kernel<T, 1><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
-    case 2: wavespeed_kernel<T, 2><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
-    default: wavespeed_kernel<T, 3><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, accum, ctrl); break;
+    case 1: wavespeed_kernel<T, 1><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, (T)pinf, accum, ctrl); break;
+    case 2: wavespeed_kernel<T, 2><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, (T)pinf, accum, ctrl); break;
+    default: wavespeed_kernel<T, 3><<<(unsigned)blocks, 256, 0, st>>>(p, g->pitch, cells, (T)gamma, (T)pinf, accum, ctrl); break;
   }
   return cudaGetLastError();
 }
@@ -174,26 +183,29 @@ __global__ void fill_riemann_kernel(T* __restrict__ out, int64_t pitch, int64_t 
 }
 
 template <typename T>
-void prim_to_cons_host(int D, const double* prim_d, T gamma, T* cons) {
-  // state_impl.hpp:390-406 (energy 136-142, eos ideal_gas.hpp:59-63)
+void prim_to_cons_host(int D, const double* prim_d, T gamma, T pinf, T* cons) {
+  // state_impl.hpp:390-406 (energy 136-142, eos ideal_gas.hpp:59-63 and
+  // stiff_fluid.hpp:76-80: e = (p + gamma p_inf) / ((gamma - 1) rho); p_inf = 0
+  // gives the ideal gas's value exactly)
   T prim[5];
   for (int k = 0; k < D + 2; ++k) prim[k] = (T)prim_d[k];
   // host code is compiled with -ffp-contract=off: every product is rounded
   T v2 = T(0);
   for (int d = 0; d < D; ++d) v2 += prim[2 + d] * prim[2 + d];
-  const T e = prim[1] / ((gamma - T(1)) * prim[0]);
+  const T e = (prim[1] + gamma * pinf) / ((gamma - T(1)) * prim[0]);
   cons[0] = prim[0];
   cons[1] = prim[0] * (T(0.5) * v2 + e);
   for (int d = 0; d < D; ++d) cons[2 + d] = prim[2 + d] * prim[0];
 }
 
 template <typename T>
-cudaError_t launch_fill(const fl_grid* g, const double* states, double gamma, void* out,
-                        cudaStream_t st) {
+cudaError_t launch_fill(const fl_grid* g, const double* states, double gamma, double pinf,
+                        void* out, cudaStream_t st) {
   RiemannStates<T> rs;
   memset(&rs, 0, sizeof(rs));
   const int D = g->dims;
-  for (int s = 0; s < (1 << D); ++s) prim_to_cons_host<T>(D, states + s * (D + 2), (T)gamma, rs.s[s]);
+  for (int s = 0; s < (1 << D); ++s)
+    prim_to_cons_host<T>(D, states + s * (D + 2), (T)gamma, (T)pinf, rs.s[s]);
   const int64_t cells = g->n[0] * g->n[1] * g->n[2];
   int64_t blocks = (cells + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
@@ -272,6 +284,7 @@ struct fl_sim {
   fl::Policy pol;
   uint32_t policy;
   double gamma;
+  double pinf;             // stiffened fluid's p_inf (0: ideal gas)
   uint32_t boundary;
   int device;
   fl::StepControl* ctrl;   // device
@@ -297,20 +310,20 @@ int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy) {
   return (int64_t)(grid->dims + 2) * grid->pitch * (int64_t)elem_size(decode(policy));
 }
 
-int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out, double gamma,
-                   double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,
-                   void* stream) {
+int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
+                       const fl_material* mat, double dtdh, uint32_t policy,
+                       uint32_t boundary_mask, double* max_ws_out, void* stream) {
   int rc = check_grid(grid);
   if (rc) return rc;
   if ((rc = check_policy(policy))) return rc;
   if (dim < 0 || dim >= grid->dims) return fail(kEInval, "dim %d out of range", dim);
   if (in == nullptr || out == nullptr) return fail(kEInval, "NULL state buffer");
   if (in == out) return fail(kEInval, "in and out must differ");
-  if (!(gamma > 1.0)) return fail(kEInval, "gamma must exceed 1");
+  if ((rc = check_material(mat))) return rc;
   if (boundary_mask >> grid->dims) return fail(kEInval, "boundary_mask has bits beyond dims");
   const Policy pol = decode(policy);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  SweepParams p = make_params(grid, pol, gamma, dtdh, boundary_mask);
+  SweepParams p = make_params(grid, pol, mat->gamma, mat->p_inf, dtdh, boundary_mask);
   p.in = in;
   p.out = out;
   if (max_ws_out != nullptr) {
@@ -323,15 +336,24 @@ int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out, doub
   return kOk;
 }
 
-int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma, double dtdh,
-                   uint32_t policy, uint32_t boundary_mask, double* max_ws_out, void* stream) {
+int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out, double gamma,
+                   double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,
+                   void* stream) {
+  const fl_material mat{gamma, 0.0};
+  return fl_split_sweep_mat(grid, dim, in, out, &mat, dtdh, policy, boundary_mask, max_ws_out,
+                            stream);
+}
+
+int fl_split_solve_mat(const fl_grid* grid, void** in, void** out, const fl_material* mat,
+                       double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,
+                       void* stream) {
   if (in == nullptr || out == nullptr) return fail(kEInval, "NULL buffer handle");
   int rc = check_grid(grid);
   if (rc) return rc;
   // split_solver.cuh:67-79: sweep x, y, z; swap between sweeps
   for (int d = 0; d < grid->dims; ++d) {
     double* ws = (d == grid->dims - 1) ? max_ws_out : nullptr;
-    rc = fl_split_sweep(grid, d, *in, *out, gamma, dtdh, policy, boundary_mask, ws, stream);
+    rc = fl_split_sweep_mat(grid, d, *in, *out, mat, dtdh, policy, boundary_mask, ws, stream);
     if (rc) return rc;
     if (grid->dims != 1 && d < grid->dims - 1) {
       void* t = *in;
@@ -342,33 +364,55 @@ int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma, dou
   return kOk;
 }
 
-int fl_max_wavespeed(const fl_grid* grid, const void* in, double gamma, uint32_t policy,
-                     double* max_ws_out, void* stream) {
+int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma, double dtdh,
+                   uint32_t policy, uint32_t boundary_mask, double* max_ws_out, void* stream) {
+  const fl_material mat{gamma, 0.0};
+  return fl_split_solve_mat(grid, in, out, &mat, dtdh, policy, boundary_mask, max_ws_out, stream);
+}
+
+int fl_max_wavespeed_mat(const fl_grid* grid, const void* in, const fl_material* mat,
+                         uint32_t policy, double* max_ws_out, void* stream) {
   int rc = check_grid(grid);
   if (rc) return rc;
   if ((rc = check_policy(policy))) return rc;
+  if ((rc = check_material(mat))) return rc;
   if (in == nullptr || max_ws_out == nullptr) return fail(kEInval, "NULL pointer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(max_ws_out, 0, sizeof(double), st);
   if (e != cudaSuccess) return cuda_fail(e, "fl_max_wavespeed");
   auto* acc = reinterpret_cast<unsigned long long*>(max_ws_out);
-  e = decode(policy).f32 ? launch_wavespeed<float>(grid, in, gamma, acc, nullptr, st)
-                         : launch_wavespeed<double>(grid, in, gamma, acc, nullptr, st);
+  const double g = mat->gamma, pi = mat->p_inf;
+  e = decode(policy).f32 ? launch_wavespeed<float>(grid, in, g, pi, acc, nullptr, st)
+                         : launch_wavespeed<double>(grid, in, g, pi, acc, nullptr, st);
   if (e != cudaSuccess) return cuda_fail(e, "fl_max_wavespeed");
+  return kOk;
+}
+
+int fl_max_wavespeed(const fl_grid* grid, const void* in, double gamma, uint32_t policy,
+                     double* max_ws_out, void* stream) {
+  const fl_material mat{gamma, 0.0};
+  return fl_max_wavespeed_mat(grid, in, &mat, policy, max_ws_out, stream);
+}
+
+int fl_fill_riemann_mat(const fl_grid* grid, const double* states_prim, const fl_material* mat,
+                        uint32_t policy, void* out, void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  if ((rc = check_policy(policy))) return rc;
+  if ((rc = check_material(mat))) return rc;
+  if (states_prim == nullptr || out == nullptr) return fail(kEInval, "NULL pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const double g = mat->gamma, pi = mat->p_inf;
+  cudaError_t e = decode(policy).f32 ? launch_fill<float>(grid, states_prim, g, pi, out, st)
+                                     : launch_fill<double>(grid, states_prim, g, pi, out, st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_fill_riemann");
   return kOk;
 }
 
 int fl_fill_riemann(const fl_grid* grid, const double* states_prim, double gamma,
                     uint32_t policy, void* out, void* stream) {
-  int rc = check_grid(grid);
-  if (rc) return rc;
-  if ((rc = check_policy(policy))) return rc;
-  if (states_prim == nullptr || out == nullptr) return fail(kEInval, "NULL pointer");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaError_t e = decode(policy).f32 ? launch_fill<float>(grid, states_prim, gamma, out, st)
-                                     : launch_fill<double>(grid, states_prim, gamma, out, st);
-  if (e != cudaSuccess) return cuda_fail(e, "fl_fill_riemann");
-  return kOk;
+  const fl_material mat{gamma, 0.0};
+  return fl_fill_riemann_mat(grid, states_prim, &mat, policy, out, stream);
 }
 
 int fl_aos_to_soa(const fl_grid* grid, uint32_t policy, const void* aos, void* soa,
@@ -469,8 +513,8 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res, double s
     base = static_cast<const char*>(a) + sim->own_lo * row_cells * (int64_t)elem_size(sim->pol);
   }
   StepControl* fin = sim->external ? nullptr : sim->ctrl;
-  e = sim->pol.f32 ? launch_wavespeed<float>(&view, base, sim->gamma, acc, fin, st)
-                   : launch_wavespeed<double>(&view, base, sim->gamma, acc, fin, st);
+  e = sim->pol.f32 ? launch_wavespeed<float>(&view, base, sim->gamma, sim->pinf, acc, fin, st)
+                   : launch_wavespeed<double>(&view, base, sim->gamma, sim->pinf, acc, fin, st);
   if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
   return kOk;
 }
@@ -482,7 +526,7 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
   if (sim->cursor != 0) return fail(kEInval, "a step is half done (fl_sim_sweep)");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int D = sim->grid.dims;
-  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, 0.0, sim->boundary);
+  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, sim->pinf, 0.0, sim->boundary);
   p.ctrl = sim->ctrl;
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;
@@ -508,6 +552,15 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
     }
     sim->enqueued += 1;
   }
+  return kOk;
+}
+
+int fl_sim_set_material(fl_sim* sim, const fl_material* mat) {
+  if (sim == nullptr) return fail(kEInval, "sim is NULL");
+  int rc = check_material(mat);
+  if (rc) return rc;
+  sim->gamma = mat->gamma;
+  sim->pinf = mat->p_inf;
   return kOk;
 }
 
@@ -548,7 +601,7 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
     si = so;
     so = t;
   }
-  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, 0.0, sim->boundary);
+  SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, sim->pinf, 0.0, sim->boundary);
   p.ctrl = sim->ctrl;
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;

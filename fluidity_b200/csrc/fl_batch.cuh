@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(WalkCfg<T, S>::THREADS) batch2d_kernel(BatchAr
   p.n[1] = pr.n1;
   p.n[2] = 1;
   p.gamma = a.gamma;
+  p.pinf = 0.0;                                      // batched problems are ideal gases
   p.dtdh = 0.0;
   p.limiter = a.limiter;
   p.basic = a.basic;

@@ -35,6 +35,7 @@ struct SweepParams {
   int64_t pitch;          // elements between component planes
   int64_t n[3];           // cells per dimension (x fastest); unused = 1
   double gamma;
+  double pinf;            // stiffened fluid's p_inf; kernels read it when FLUX has kStiffEos
   double dtdh;            // used when ctrl == nullptr
   int limiter;            // LimiterKind
   int basic;              // 1: piecewise-constant reconstruction

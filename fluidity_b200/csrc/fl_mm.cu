@@ -43,6 +43,7 @@ struct MMArgs {
   int64_t nx, ny, pitch;
   double h;
   double gamma[2];
+  double pinf[2];       // stiffened fluids' p_inf (0: ideal gas)
   const void* u[2];     // states (read by the scan)
   void* w[2];           // states (written by scatter / extrapolation)
   void* x[2];           // second buffers (Jacobi ping-pong)
@@ -87,10 +88,12 @@ __device__ __forceinline__ double wavespeed_slr(const double* u, double pstar, d
 }
 
 // Hllc::solve_star_conservative_left (flux_method/flux_hllc.hpp:330-361) with
-// two equations of state, normal direction x.
-__device__ void star_left(const double* ul, const double* ur, double gl, double gr, double* out) {
+// two equations of state, normal direction x.  Sound speeds take each side's
+// p_inf (stiff_fluid.hpp:92-96; 0 for the ideal gas: p + 0 = p).
+__device__ void star_left(const double* ul, const double* ur, double gl, double gr, double il,
+                          double ir, double* out) {
   const double pl = pressure2(ul, gl), pr = pressure2(ur, gr);
-  const double al = sqrt(gl * pl / ul[0]), ar = sqrt(gr * pr / ur[0]);
+  const double al = sqrt(gl * (pl + il) / ul[0]), ar = sqrt(gr * (pr + ir) / ur[0]);
   const double vl = ul[2] / ul[0], vr = ur[2] / ur[0];
   const double p_pvrs = 0.5 * ((pl + pr) - (0.25 * (vr - vl) * (ur[0] + ul[0]) * (al + ar)));
   const double p_star = dmaxr(0.0, p_pvrs);
@@ -160,7 +163,7 @@ __device__ bool gfm_source(const double* pa, const double* pb, int64_t nx, int64
 template <typename T>
 __device__ void gfm_star(const T* ua, const T* ub, int64_t pitch, int64_t nx, int64_t ny,
                          const double* pa, int64_t x, int64_t y, double h, const double* n,
-                         double ga, double gb, double* star) {
+                         double ga, double gb, double ia, double ib, double* star) {
   const double abs_phi = fabs(pa[y * nx + x]);
   const double h32 = 1.5 * h;
   double w[2], wl[4], wr[4];
@@ -179,7 +182,7 @@ __device__ void gfm_star(const T* ua, const T* ub, int64_t pitch, int64_t nx, in
   wr[2] = vr_n * wr[0];
   wl[3] = 0.0 * wl[0];
   wr[3] = 0.0 * wr[0];
-  star_left(wl, wr, ga, gb, star);
+  star_left(wl, wr, ga, gb, ia, ib, star);
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
     const double sv = star[2 + d] / star[0];
@@ -232,7 +235,8 @@ __global__ void __launch_bounds__(256) mm_scan_kernel(MMArgs a) {
       if (!found) continue;
       double star[4];
       gfm_star(static_cast<const T*>(a.u[m]), static_cast<const T*>(a.u[1 - m]), a.pitch, a.nx,
-               a.ny, pa, sx, sy, a.h, nrm, a.gamma[m], a.gamma[1 - m], star);
+               a.ny, pa, sx, sy, a.h, nrm, a.gamma[m], a.gamma[1 - m], a.pinf[m], a.pinf[1 - m],
+               star);
       const int slot = atomicAdd(&a.cnt->gfm[m], 1);
       a.gfm_idx[m][slot] = (int)t;
 #pragma unroll
@@ -402,6 +406,7 @@ struct fl_mm {
   uint32_t policy;
   bool f32;
   double gamma[2];
+  double pinf[2];   // stiffened fluids' p_inf (0: ideal gas)
   double h;
   // owned device workspace
   MMCounters* cnt;
@@ -455,6 +460,7 @@ int ghost_pass(fl_mm* m, void* const* u, void* const* x, const double* const* ph
   a.h = m->h;
   for (int k = 0; k < 2; ++k) {
     a.gamma[k] = m->gamma[k];
+    a.pinf[k] = m->pinf[k];
     a.u[k] = u[k];
     a.w[k] = u[k];
     a.x[k] = x[k];
@@ -557,22 +563,25 @@ int fl_mm_stats(const fl_mm* m, int32_t* out, int32_t n) {
   return kOk;
 }
 
-int fl_mm_set_states(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
-                     const double* prim, double gamma, void* stream) {
+int fl_mm_set_states_mat(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
+                         const double* prim, const fl_material* mat, void* stream) {
   int rc = check_mm_grid(grid);
   if (rc) return rc;
-  if (!state || !phi || !prim) return set_error(kEInval, "NULL pointer");
+  if (!state || !phi || !prim || !mat) return set_error(kEInval, "NULL pointer");
+  const double gamma = mat->gamma, pinf = mat->p_inf;
   if (!(gamma > 1.0)) return set_error(kEInval, "gamma must exceed 1");
+  if (!(pinf >= 0.0) || pinf > DBL_MAX) return set_error(kEInval, "p_inf must be finite and >= 0");
   const int64_t n = grid->n[0] * grid->n[1];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // prim -> cons in the state's precision (state/state_impl.hpp:390-406)
   if (policy & 1u) {
     const float r = (float)prim[0], p = (float)prim[1], vx = (float)prim[2], vy = (float)prim[3];
-    const float g = (float)gamma;
+    const float g = (float)gamma, pi = (float)pinf;
     float v2 = 0.0f;
     v2 += vx * vx;
     v2 += vy * vy;
-    const float e = p / ((g - 1.0f) * r);
+    // e from the eos (ideal_gas.hpp:59-63; stiff_fluid.hpp:76-80)
+    const float e = (p + g * pi) / ((g - 1.0f) * r);
     set_states_kernel<float><<<grid_for(n), 256, 0, st>>>(static_cast<float*>(state), grid->pitch,
                                                           n, phi, r, r * (0.5f * v2 + e), vx * r,
                                                           vy * r);
@@ -581,13 +590,33 @@ int fl_mm_set_states(const fl_grid* grid, uint32_t policy, void* state, const do
     double v2 = 0.0;
     v2 += vx * vx;
     v2 += vy * vy;
-    const double e = p / ((gamma - 1.0) * r);
+    const double e = (p + gamma * pinf) / ((gamma - 1.0) * r);
     set_states_kernel<double><<<grid_for(n), 256, 0, st>>>(static_cast<double*>(state),
                                                            grid->pitch, n, phi, r,
                                                            r * (0.5 * v2 + e), vx * r, vy * r);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "fl_mm_set_states");
+  return kOk;
+}
+
+int fl_mm_set_states(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
+                     const double* prim, double gamma, void* stream) {
+  const fl_material mat{gamma, 0.0};
+  return fl_mm_set_states_mat(grid, policy, state, phi, prim, &mat, stream);
+}
+
+int fl_mm_set_materials(fl_mm* m, const fl_material* mats) {
+  if (m == nullptr || mats == nullptr) return set_error(kEInval, "NULL pointer");
+  for (int k = 0; k < 2; ++k) {
+    if (!(mats[k].gamma > 1.0)) return set_error(kEInval, "gamma of material %d must exceed 1", k);
+    if (!(mats[k].p_inf >= 0.0) || mats[k].p_inf > DBL_MAX)
+      return set_error(kEInval, "p_inf of material %d must be finite and >= 0", k);
+  }
+  for (int k = 0; k < 2; ++k) {
+    m->gamma[k] = mats[k].gamma;
+    m->pinf[k] = mats[k].p_inf;
+  }
   return kOk;
 }
 
@@ -655,7 +684,8 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     if (rc) return rc;
     // 3: time step over both materials (multimaterial_simulator.hpp:384-404)
     for (int mat = 0; mat < 2; ++mat) {
-      rc = fl_max_wavespeed(g, u[mat], m->gamma[mat], m->policy, m->ws_dev + mat, stream);
+      const fl_material mm{m->gamma[mat], m->pinf[mat]};
+      rc = fl_max_wavespeed_mat(g, u[mat], &mm, m->policy, m->ws_dev + mat, stream);
       if (rc) return rc;
     }
     double ws[2];
@@ -674,7 +704,8 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     for (int mat = 0; mat < 2; ++mat) {
       void* in = m->u[mat][0];
       void* out = m->u[mat][1];
-      rc = fl_split_solve(g, &in, &out, m->gamma[mat], dtdh, m->policy, 0u, nullptr, stream);
+      const fl_material mm{m->gamma[mat], m->pinf[mat]};
+      rc = fl_split_solve_mat(g, &in, &out, &mm, dtdh, m->policy, 0u, nullptr, stream);
       if (rc) return rc;
     }
     // 5: level sets (multimaterial_simulator.hpp:428-477)

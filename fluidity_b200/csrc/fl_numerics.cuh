@@ -24,6 +24,9 @@
 namespace fl {
 
 enum FluxKind : int { kHllc = 0, kForce = 1, kLaxFriedrichs = 2, kRichtmyer = 3 };
+// Added to a FLUX template argument: the material is the stiffened fluid
+// (material/stiff_fluid.hpp:38-133) rather than the ideal gas.
+constexpr int kStiffEos = 4;
 enum LimiterKind : int { kVanLeer = 0, kSuperbee = 1 };
 
 template <typename T> FL_HD T fl_sqrt(T x);
@@ -80,19 +83,35 @@ FL_HD void flux(const Cons<T, D>& u, int d, T gamma,
   flux_vp(u, d, velocity(u, d), pressure(u, gamma), f);
 }
 
-// sqrt(gamma p / rho) (material/ideal_gas.hpp:75-78)
+// The pressure under the sound speed's root: p for the ideal gas
+// (material/ideal_gas.hpp:75-78), p + p_inf for the stiffened fluid
+// (material/stiff_fluid.hpp:92-96).  For both materials the state's pressure
+// is (gamma - 1)(E - rho |v|^2 / 2) (state_impl.hpp:117-128): the reference
+// subtracts no gamma p_inf there, so a stiffened fluid's energy, filled with
+// e = (p + gamma p_inf) / ((gamma - 1) rho), reads back as p + gamma p_inf.
+template <bool STIFF, typename T>
+FL_HD T sound_p(T p, T pinf) {
+  if constexpr (STIFF) {
+    return p + pinf;
+  } else {
+    return p;
+  }
+}
+
+// sqrt(gamma p / rho) (material/ideal_gas.hpp:75-78); the caller passes
+// sound_p's pressure
 template <typename T, int D>
 FL_HD T sound_speed_p(const Cons<T, D>& u, T gamma, T p) {
   return fl_sqrt<T>(gamma * p / u.v[0]);
 }
 
 // max_d |u_d| + a (state_impl.hpp:167-178)
-template <typename T, int D>
-FL_HD T max_wavespeed(const Cons<T, D>& u, T gamma) {
+template <bool STIFF = false, typename T, int D>
+FL_HD T max_wavespeed(const Cons<T, D>& u, T gamma, T pinf = T(0)) {
   T m = fl_abs<T>(velocity(u, 0));
 #pragma unroll
   for (int d = 1; d < D; ++d) m = std_max(m, fl_abs<T>(velocity(u, d)));
-  return m + sound_speed_p(u, gamma, pressure(u, gamma));
+  return m + sound_speed_p(u, gamma, sound_p<STIFF>(pressure(u, gamma), pinf));
 }
 
 // ---- HLLC (flux_method/flux_hllc.hpp:56-245) ---------------------------
@@ -108,13 +127,13 @@ FL_HD void hllc_star(const Cons<T, D>& u, int d, T s, T sstar,
   out.v[1] = scale * (u.v[1] + u.v[0] * (sstar - vel) * (sstar + p / (u.v[0] * sf)));
 }
 
-template <typename T, int D>
+template <bool STIFF = false, typename T, int D>
 FL_HD void hllc(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
-                                     T gamma, Cons<T, D>& f) {
+                                     T gamma, Cons<T, D>& f, T pinf = T(0)) {
   const T pl = pressure(ul, gamma), pr = pressure(ur, gamma);
   const T vl = velocity(ul, d), vr = velocity(ur, d);
-  const T al = sound_speed_p(ul, gamma, pl);
-  const T ar = sound_speed_p(ur, gamma, pr);
+  const T al = sound_speed_p(ul, gamma, sound_p<STIFF>(pl, pinf));
+  const T ar = sound_speed_p(ur, gamma, sound_p<STIFF>(pr, pinf));
   const T adi = (gamma + T(1)) / (T(2) * gamma);
   const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * (vr - vl) * (ur.v[0] + ul.v[0]) * (al + ar)));
   const T p_star = std_max(T(0), p_pvrs);
@@ -168,18 +187,21 @@ FL_HD void richtmyer_ff(const Cons<T, D>& ul, const Cons<T, D>& ur,
   flux(u, d, gamma, f);
 }
 
+// FLUX: a FluxKind, plus kStiffEos for the stiffened fluid's sound speed
+// (which only HLLC uses; p_inf is ignored otherwise).
 template <int FLUX, typename T, int D>
 FL_HD void riemann(const Cons<T, D>& ul, const Cons<T, D>& ur, int d,
-                                        T gamma, T dtdh, Cons<T, D>& f) {
-  if constexpr (FLUX == kHllc) {
-    hllc(ul, ur, d, gamma, f);
+                                        T gamma, T dtdh, Cons<T, D>& f, T pinf = T(0)) {
+  constexpr int RS = FLUX & 3;
+  if constexpr (RS == kHllc) {
+    hllc<(FLUX & kStiffEos) != 0>(ul, ur, d, gamma, f, pinf);
   } else {
     Cons<T, D> fl, fr;
     flux(ul, d, gamma, fl);
     flux(ur, d, gamma, fr);
-    if constexpr (FLUX == kLaxFriedrichs) {
+    if constexpr (RS == kLaxFriedrichs) {
       lax_friedrichs_ff(ul, ur, fl, fr, dtdh, f);
-    } else if constexpr (FLUX == kRichtmyer) {
+    } else if constexpr (RS == kRichtmyer) {
       richtmyer_ff(ul, ur, fl, fr, d, gamma, dtdh, f);
     } else {
       Cons<T, D> a, b;
@@ -347,23 +369,23 @@ FL_HD void flux_q(const Cons<T, D>& u, const Derived<T, D>& q, int d,
   flux_vp(u, d, q.v[d], q.p, f);
 }
 
-// max_d |u_d| + sqrt(gamma p / rho)
-template <typename T, int D>
-FL_HD T max_wavespeed_q(const Derived<T, D>& q, T gamma) {
+// max_d |u_d| + sqrt(gamma p / rho); p + p_inf under the root when STIFF
+template <bool STIFF = false, typename T, int D>
+FL_HD T max_wavespeed_q(const Derived<T, D>& q, T gamma, T pinf = T(0)) {
   T m = fl_abs<T>(q.v[0]);
 #pragma unroll
   for (int d = 1; d < D; ++d) m = std_max(m, fl_abs<T>(q.v[d]));
-  return m + fl_ksqrt<T>(gamma * q.p * q.rinv);
+  return m + fl_ksqrt<T>(gamma * sound_p<STIFF>(q.p, pinf) * q.rinv);
 }
 
 // HLLC with precomputed side quantities; adi = (gamma + 1) / (2 gamma).
-template <typename T, int D>
+template <bool STIFF = false, typename T, int D>
 FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
                                        const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
-                                       T gamma, T adi, Cons<T, D>& f) {
+                                       T gamma, T adi, Cons<T, D>& f, T pinf = T(0)) {
   const T pl = ql.p, pr = qr.p, vl = ql.v[d], vr = qr.v[d];
-  const T al = fl_ksqrt<T>(gamma * pl * ql.rinv);
-  const T ar = fl_ksqrt<T>(gamma * pr * qr.rinv);
+  const T al = fl_ksqrt<T>(gamma * sound_p<STIFF>(pl, pinf) * ql.rinv);
+  const T ar = fl_ksqrt<T>(gamma * sound_p<STIFF>(pr, pinf) * qr.rinv);
   const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * (vr - vl) * (ur.v[0] + ul.v[0]) * (al + ar)));
   const T p_star = std_max(T(0), p_pvrs);
   const T wsl = (p_star <= pl) ? vl + (-al)
@@ -403,28 +425,31 @@ FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
   for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + s * (st.v[c] - u.v[c]);
 }
 
+// FLUX as for riemann.
 template <int FLUX, typename T, int D>
 FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
                                           const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
-                                          T gamma, T gm1, T adi, T dtdh, Cons<T, D>& f) {
-  if constexpr (FLUX == kHllc) {
-    hllc_q(ul, ql, ur, qr, d, gamma, adi, f);
+                                          T gamma, T gm1, T adi, T dtdh, Cons<T, D>& f,
+                                          T pinf = T(0)) {
+  constexpr int RS = FLUX & 3;
+  if constexpr (RS == kHllc) {
+    hllc_q<(FLUX & kStiffEos) != 0>(ul, ql, ur, qr, d, gamma, adi, f, pinf);
   } else {
     Cons<T, D> fl, fr;
     flux_q(ul, ql, d, fl);
     flux_q(ur, qr, d, fr);
     Cons<T, D> lf, ri;
-    if constexpr (FLUX != kRichtmyer) lax_friedrichs_ff(ul, ur, fl, fr, dtdh, lf);
-    if constexpr (FLUX != kLaxFriedrichs) {
+    if constexpr (RS != kRichtmyer) lax_friedrichs_ff(ul, ur, fl, fr, dtdh, lf);
+    if constexpr (RS != kLaxFriedrichs) {
       Cons<T, D> m;
 #pragma unroll
       for (int c = 0; c < D + 2; ++c)
         m.v[c] = T(0.5) * (ul.v[c] + ur.v[c] + dtdh * (fl.v[c] - fr.v[c]));
       flux_q(m, derive(m, gm1), d, ri);
     }
-    if constexpr (FLUX == kLaxFriedrichs) {
+    if constexpr (RS == kLaxFriedrichs) {
       f = lf;
-    } else if constexpr (FLUX == kRichtmyer) {
+    } else if constexpr (RS == kRichtmyer) {
       f = ri;
     } else {
 #pragma unroll

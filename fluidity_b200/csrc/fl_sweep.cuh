@@ -162,7 +162,9 @@ sweep_kernel(SweepParams p) {
 
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
   const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
+  constexpr bool STIFF = (FLUX & kStiffEos) != 0;
   const T gamma = (T)p.gamma;
+  const T pinf = (T)p.pinf;
   const T gm1 = gamma - T(1);
   const T adi = (gamma + T(1)) / (T(2) * gamma);
 
@@ -316,7 +318,8 @@ sweep_kernel(SweepParams p) {
       ul.v[c] = sER[c * G::E + el_idx];
       ur.v[c] = sEL[c * G::E + el_idx + ES];
     }
-    riemann_q<FLUX>(ul, derive(ul, gm1), ur, derive(ur, gm1), S, gamma, gm1, adi, dtdh, fx);
+    riemann_q<FLUX>(ul, derive(ul, gm1), ur, derive(ur, gm1), S, gamma, gm1, adi, dtdh, fx,
+                    pinf);
 #pragma unroll
     for (int c = 0; c < NC; ++c) sFX[c * G::F + f] = fx.v[c];
   }
@@ -342,7 +345,7 @@ sweep_kernel(SweepParams p) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
     if (want_ws && ws_row_counts(p, D == 1 ? g0 : (D == 2 ? g1 : g2)))
-      ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+      ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
   }
   if (want_ws)
     cta_wavespeed_commit<NT>(ws_local, p.ws_accum, p.ctrl, p.finalize, true, s_red);

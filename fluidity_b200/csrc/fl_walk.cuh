@@ -79,7 +79,9 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
   using W = WalkCfg<T, S>;
   constexpr int D = 2;
   constexpr int NC = 4;
+  constexpr bool STIFF = (FLUX & kStiffEos) != 0;
   const T gamma = (T)p.gamma;
+  const T pinf = (T)p.pinf;
   const T gm1 = gamma - T(1);
   const T adi = (gamma + T(1)) / (T(2) * gamma);
   const T hd = T(0.5) * dtdh;
@@ -208,7 +210,8 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
         Cons<T, D> ul, fx_l;
 #pragma unroll
         for (int c = 0; c < NC; ++c) ul.v[c] = shfl_up(er.v[c], 1);
-        riemann_q<FLUX>(ul, derive(ul, gm1), el, derive(el, gm1), 0, gamma, gm1, adi, dtdh, fx_l);
+        riemann_q<FLUX>(ul, derive(ul, gm1), el, derive(el, gm1), 0, gamma, gm1, adi, dtdh, fx_l,
+                        pinf);
         Cons<T, D> r;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -220,14 +223,14 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
 #pragma unroll
           for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
           if (want_ws && ws_row_counts(p, j))
-            ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+            ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
         }
       } else {
         if (j >= y0) {
           // face (j-1, j) along y, then update of row j - 1
           Cons<T, D> fxy;
           riemann_q<FLUX>(er_prev, derive(er_prev, gm1), el, derive(el, gm1), 1, gamma, gm1,
-                          adi, dtdh, fxy);
+                          adi, dtdh, fxy, pinf);
           if (j >= y0 + 1 && owned) {
             const Cons<T, D>& uo = U[0];
             Cons<T, D> r;
@@ -237,7 +240,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
 #pragma unroll
             for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
             if (want_ws && ws_row_counts(p, j - 1))
-              ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+              ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
           }
           f_prev = fxy;
         }

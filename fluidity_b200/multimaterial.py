@@ -2,7 +2,8 @@
 
 Mirrors the reference's MultimaterialSimulator
 (simulator/multimaterial_simulator.hpp): two materials share a 2-D grid, each
-with its own state buffers, ideal-gas gamma and FP64 level set; a step loads
+with its own state buffers, equation of state (ideal gas, or the stiffened
+fluid when its p_inf > 0) and FP64 level set; a step loads
 the ghost cells (Riemann GFM + extrapolation), takes one CFL time step over
 both materials, advances each material with the split solver and moves,
 projects and reinitialises the level sets.  Device buffers are torch tensors
@@ -23,7 +24,7 @@ _DT = {"f64": torch.float64, "f32": torch.float32}
 
 class MultiMaterial:
     def __init__(self, shape, gammas, res: float, dtype: str = "f32", flux: str = "hllc",
-                 limiter: str = "vanleer", device="cuda"):
+                 limiter: str = "vanleer", device="cuda", p_infs=(0.0, 0.0)):
         if len(shape) != 2:
             raise ValueError("the two-material path is 2-D")
         self.shape = tuple(int(v) for v in shape)
@@ -31,6 +32,8 @@ class MultiMaterial:
         self.dtype = dtype
         self.res = float(res)
         self.gammas = (float(gammas[0]), float(gammas[1]))
+        self.p_infs = (float(p_infs[0]), float(p_infs[1]))
+        self.materials = [capi.Material(g, p) for g, p in zip(self.gammas, self.p_infs)]
         self.policy = capi.policy_bits(dtype, flux, limiter)
         self.grid = capi.Grid.make(self.shape)
         self.lib = capi.load()
@@ -39,6 +42,9 @@ class MultiMaterial:
         capi.check(self.lib.fl_mm_create(C.byref(h), C.byref(self.grid), g, self.policy,
                                          self.res), self.lib)
         self.handle = h
+        if any(self.p_infs):
+            mats = (capi.Material * 2)(*self.materials)
+            capi.check(self.lib.fl_mm_set_materials(h, mats), self.lib)
         dev = torch.device(device)
         self.u = [[torch.zeros((4, self.cells), dtype=_DT[dtype], device=dev) for _ in range(2)]
                   for _ in range(2)]
@@ -62,10 +68,11 @@ class MultiMaterial:
         pr = (C.c_double * 4)(*[float(v) for v in prim])
         phi_t = phi if isinstance(phi, torch.Tensor) else torch.tensor(
             np.ascontiguousarray(phi, dtype=np.float64), device=self.u[0][0].device)
-        rc = self.lib.fl_mm_set_states(C.byref(self.grid), self.policy,
-                                       C.c_void_p(self.u[material][0].data_ptr()),
-                                       C.c_void_p(phi_t.data_ptr()), pr, self.gammas[material],
-                                       _stream_ptr(stream))
+        rc = self.lib.fl_mm_set_states_mat(C.byref(self.grid), self.policy,
+                                           C.c_void_p(self.u[material][0].data_ptr()),
+                                           C.c_void_p(phi_t.data_ptr()), pr,
+                                           C.byref(self.materials[material]),
+                                           _stream_ptr(stream))
         capi.check(rc, self.lib)
 
     def set_levelsets(self, phi0, phi1):

@@ -40,15 +40,22 @@ def state_tensor(shape, dtype: str = "f64", device="cuda", pitch: int | None = N
 
 
 class SplitSolver:
-    """Dimensionally split MUSCL-Hancock / HLLC|FORCE step on one GPU."""
+    """Dimensionally split MUSCL-Hancock / HLLC|FORCE step on one GPU.
+
+    p_inf = 0 is the ideal gas (material/ideal_gas.hpp); p_inf > 0 the
+    stiffened fluid StiffFluid(gamma, p_inf) (material/stiff_fluid.hpp:38-133),
+    through the C ABI's fl_material entry points."""
 
     def __init__(self, shape, dtype: str = "f64", flux: str = "hllc",
                  limiter: str = "vanleer", recon: str = "muscl", gamma: float = 1.4,
-                 boundary_mask: int = 0, flatten: bool = True, pitch: int | None = None):
+                 boundary_mask: int = 0, flatten: bool = True, pitch: int | None = None,
+                 p_inf: float = 0.0):
         self.shape = tuple(int(v) for v in shape)
         self.dims = len(self.shape)
         self.dtype = dtype
         self.gamma = float(gamma)
+        self.p_inf = float(p_inf)
+        self.material = capi.Material(self.gamma, self.p_inf)
         self.boundary_mask = int(boundary_mask)
         self.policy = capi.policy_bits(dtype, flux, limiter, recon, flatten)
         self.grid = capi.Grid.make(self.shape, pitch)
@@ -60,30 +67,45 @@ class SplitSolver:
     def sweep(self, src, dst, dim: int, dtdh: float, max_ws=None, stream=None):
         """One dimensional sweep; max_ws (1-element float64 cuda tensor) receives
         the max wavespeed of dst."""
-        rc = self.lib.fl_split_sweep(C.byref(self.grid), int(dim), C.c_void_p(src.data_ptr()),
-                                     C.c_void_p(dst.data_ptr()), self.gamma, float(dtdh),
-                                     self.policy, self.boundary_mask,
-                                     None if max_ws is None else C.c_void_p(max_ws.data_ptr()),
-                                     _stream_ptr(stream))
+        ws = None if max_ws is None else C.c_void_p(max_ws.data_ptr())
+        args = (C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()))
+        if self.p_inf != 0.0:
+            rc = self.lib.fl_split_sweep_mat(C.byref(self.grid), int(dim), *args,
+                                             C.byref(self.material), float(dtdh), self.policy,
+                                             self.boundary_mask, ws, _stream_ptr(stream))
+        else:
+            rc = self.lib.fl_split_sweep(C.byref(self.grid), int(dim), *args, self.gamma,
+                                         float(dtdh), self.policy, self.boundary_mask, ws,
+                                         _stream_ptr(stream))
         capi.check(rc, self.lib)
 
     def solve(self, src, dst, dtdh: float, max_ws=None, stream=None):
         """All sweeps; returns (in, out) after the reference's swap."""
         pin = C.c_void_p(src.data_ptr())
         pout = C.c_void_p(dst.data_ptr())
-        rc = self.lib.fl_split_solve(C.byref(self.grid), C.byref(pin), C.byref(pout),
-                                     self.gamma, float(dtdh), self.policy, self.boundary_mask,
-                                     None if max_ws is None else C.c_void_p(max_ws.data_ptr()),
-                                     _stream_ptr(stream))
+        ws = None if max_ws is None else C.c_void_p(max_ws.data_ptr())
+        if self.p_inf != 0.0:
+            rc = self.lib.fl_split_solve_mat(C.byref(self.grid), C.byref(pin), C.byref(pout),
+                                             C.byref(self.material), float(dtdh), self.policy,
+                                             self.boundary_mask, ws, _stream_ptr(stream))
+        else:
+            rc = self.lib.fl_split_solve(C.byref(self.grid), C.byref(pin), C.byref(pout),
+                                         self.gamma, float(dtdh), self.policy,
+                                         self.boundary_mask, ws, _stream_ptr(stream))
         capi.check(rc, self.lib)
         by_ptr = {src.data_ptr(): src, dst.data_ptr(): dst}
         return by_ptr[pin.value], by_ptr[pout.value]
 
     def max_wavespeed(self, state, stream=None) -> torch.Tensor:
         out = torch.empty(1, dtype=torch.float64, device=state.device)
-        rc = self.lib.fl_max_wavespeed(C.byref(self.grid), C.c_void_p(state.data_ptr()),
-                                       self.gamma, self.policy, C.c_void_p(out.data_ptr()),
-                                       _stream_ptr(stream))
+        if self.p_inf != 0.0:
+            rc = self.lib.fl_max_wavespeed_mat(C.byref(self.grid), C.c_void_p(state.data_ptr()),
+                                               C.byref(self.material), self.policy,
+                                               C.c_void_p(out.data_ptr()), _stream_ptr(stream))
+        else:
+            rc = self.lib.fl_max_wavespeed(C.byref(self.grid), C.c_void_p(state.data_ptr()),
+                                           self.gamma, self.policy, C.c_void_p(out.data_ptr()),
+                                           _stream_ptr(stream))
         capi.check(rc, self.lib)
         return out
 
@@ -92,9 +114,14 @@ class SplitSolver:
         sp = np.ascontiguousarray(states_prim, dtype=np.float64).reshape(2 ** self.dims,
                                                                           self.dims + 2)
         out = self.new_state() if out is None else out
-        rc = self.lib.fl_fill_riemann(C.byref(self.grid), sp.ctypes.data_as(C.c_void_p),
-                                      self.gamma, self.policy, C.c_void_p(out.data_ptr()),
-                                      _stream_ptr(stream))
+        if self.p_inf != 0.0:
+            rc = self.lib.fl_fill_riemann_mat(C.byref(self.grid), sp.ctypes.data_as(C.c_void_p),
+                                              C.byref(self.material), self.policy,
+                                              C.c_void_p(out.data_ptr()), _stream_ptr(stream))
+        else:
+            rc = self.lib.fl_fill_riemann(C.byref(self.grid), sp.ctypes.data_as(C.c_void_p),
+                                          self.gamma, self.policy, C.c_void_p(out.data_ptr()),
+                                          _stream_ptr(stream))
         capi.check(rc, self.lib)
         return out
 
@@ -109,6 +136,8 @@ class Simulation:
         capi.check(self.lib.fl_sim_create(C.byref(h), C.byref(solver.grid), solver.gamma,
                                           solver.policy, solver.boundary_mask), self.lib)
         self.handle = h
+        if solver.p_inf != 0.0:
+            capi.check(self.lib.fl_sim_set_material(h, C.byref(solver.material)), self.lib)
         self._bufs = {}
 
     def __del__(self):
@@ -203,10 +232,10 @@ class SimulatorImpl:
 
     def __init__(self, dims: int = 1, dtype: str = "f64", flux: str = "force",
                  limiter: str = "superbee", recon: str = "muscl", gamma: float = 1.4,
-                 boundary_mask: int = 0):
+                 boundary_mask: int = 0, p_inf: float = 0.0):
         self.dims = dims
         self.kw = dict(dtype=dtype, flux=flux, limiter=limiter, recon=recon, gamma=gamma,
-                       boundary_mask=boundary_mask)
+                       boundary_mask=boundary_mask, p_inf=p_inf)
         self.res = 0.0
         self.extent = [(0.0, 1.0)] * dims
         self.sim_time = 0.0

@@ -124,6 +124,37 @@ int fl_max_wavespeed(const fl_grid* grid, const void* in, double gamma,
 int fl_fill_riemann(const fl_grid* grid, const double* states_prim,
                     double gamma, uint32_t policy, void* out, void* stream);
 
+/* ---- materials.  The entry points above take the ideal gas
+ * (material/ideal_gas.hpp) by its gamma.  The _mat forms take either of the
+ * reference's equations of state: the ideal gas (p_inf = 0) or the stiffened
+ * fluid StiffFluid (material/stiff_fluid.hpp:38-133).  For the stiffened
+ * fluid:
+ *   - the sound speed is sqrt(gamma (p + p_inf) / rho) (stiff_fluid.hpp:92-96);
+ *   - a state filled from primitives gets the internal energy
+ *     (p + gamma p_inf) / ((gamma - 1) rho) (stiff_fluid.hpp:76-80);
+ *   - the pressure of a conservative state is (gamma - 1)(E - rho |v|^2 / 2),
+ *     as for the ideal gas (state/state_impl.hpp:117-128).  The reference
+ *     subtracts no gamma p_inf there, so pressures read back from a filled
+ *     state are p + gamma p_inf.  Fluxes and flattening see that pressure.
+ * With p_inf = 0 every _mat form equals its gamma-only form bit for bit.
+ * gamma must exceed 1 and p_inf must be finite and >= 0 (else FL_EINVAL). */
+typedef struct fl_material {
+  double gamma;   /* adiabatic index */
+  double p_inf;   /* stiffened fluid's material constant; 0 for the ideal gas */
+} fl_material;
+
+int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
+                       const fl_material* mat, double dtdh, uint32_t policy,
+                       uint32_t boundary_mask, double* max_ws_out, void* stream);
+int fl_split_solve_mat(const fl_grid* grid, void** in, void** out,
+                       const fl_material* mat, double dtdh, uint32_t policy,
+                       uint32_t boundary_mask, double* max_ws_out, void* stream);
+int fl_max_wavespeed_mat(const fl_grid* grid, const void* in, const fl_material* mat,
+                         uint32_t policy, double* max_ws_out, void* stream);
+int fl_fill_riemann_mat(const fl_grid* grid, const double* states_prim,
+                        const fl_material* mat, uint32_t policy, void* out,
+                        void* stream);
+
 /* Layout adapters for the reference's AoS DeviceTensor<State, D>
  * (container/device_tensor.hpp): aos holds cells * (dims + 2) values. */
 int fl_aos_to_soa(const fl_grid* grid, uint32_t policy, const void* aos,
@@ -142,6 +173,10 @@ typedef struct fl_sim fl_sim;
 int fl_sim_create(fl_sim** sim, const fl_grid* grid, double gamma,
                   uint32_t policy, uint32_t boundary_mask);
 int fl_sim_destroy(fl_sim* sim);
+
+/* Sets the loop's material (gamma and p_inf; fl_sim_create's gamma is the
+ * ideal gas).  Call before fl_sim_begin. */
+int fl_sim_set_material(fl_sim* sim, const fl_material* mat);
 
 /* Resets the loop: buffers a (initial state) and b, cfl, resolution dh,
  * stop time and step limit; enqueues the initial wavespeed reduction. */
@@ -351,6 +386,14 @@ int fl_mm_create(fl_mm** mm, const fl_grid* grid, const double* gammas, uint32_t
                  double res);
 int fl_mm_destroy(fl_mm* mm);
 
+/* Replaces the two materials (2 entries; fl_mm_create's gammas are ideal
+ * gases): an ideal gas or a stiffened fluid per material, as the reference's
+ * add_material takes either (validation/1d_mm_shock_tube_gas_water.cu:63-80).
+ * The GFM star state uses each side's sound speed
+ * (flux_method/flux_hllc.hpp:330-361), the step and the CFL maximum each
+ * material's own. */
+int fl_mm_set_materials(fl_mm* mm, const fl_material* mats);
+
 /* Ghost cells of both materials (ghost::load_ghost_cells,
  * ghost_fluid/cuda/load_ghost_cells.cuh:74-95): RiemannGFM<3> star states
  * (ghost_fluid/riemann_ghost_fluid.hpp:50-195) written beside the interface,
@@ -372,6 +415,8 @@ int fl_mm_stats(const fl_mm* mm, int32_t* out, int32_t n);
  * (state::set_states, state/cuda/state_initialization.cuh:72-119). */
 int fl_mm_set_states(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
                      const double* prim, double gamma, void* stream);
+int fl_mm_set_states_mat(const fl_grid* grid, uint32_t policy, void* state, const double* phi,
+                         const double* prim, const fl_material* mat, void* stream);
 
 /* Cells with phi1 <= 0 copy material 1's state into u0
  * (material::combine_into_first, material/cuda/combine_materials.cuh:39-81). */

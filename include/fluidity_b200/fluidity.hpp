@@ -80,7 +80,7 @@ template <typename T, std::size_t D>
 using conservative_t = StateTag<T, D, FormType::conservative>;
 }  // namespace state
 
-// ---- material (material/ideal_gas.hpp:27-119) ----------------------------------
+// ---- materials (material/ideal_gas.hpp:27-119, material/stiff_fluid.hpp:38-133) ----
 
 namespace material {
 template <typename T>
@@ -89,8 +89,29 @@ struct IdealGas {
   constexpr IdealGas() = default;
   constexpr explicit IdealGas(T adi) : adi_index(adi) {}
   constexpr T adiabatic() const { return adi_index; }
+  constexpr T p_inf() const { return T(0); }
   T adi_index = T(1.4);
 };
+
+// Stiffened fluid: sound speed sqrt(gamma (p + p_inf) / rho), filled energy
+// (p + gamma p_inf) / ((gamma - 1) rho).  Defaults and the one-argument
+// constructor keep the reference's p_inf = 0.613 (and gamma = 5.5).
+template <typename T>
+struct StiffFluid {
+  using value_t = T;
+  constexpr StiffFluid() = default;
+  constexpr explicit StiffFluid(T adi) : adi_index(adi) {}
+  constexpr StiffFluid(T adi, T pinf) : adi_index(adi), p_inf_(pinf) {}
+  constexpr T adiabatic() const { return adi_index; }
+  constexpr T p_inf() const { return p_inf_; }
+  T adi_index = T(5.5);
+  T p_inf_ = T(0.613);
+};
+
+template <typename Mat>
+fl_material to_fl(const Mat& m) {
+  return fl_material{(double)m.adiabatic(), (double)m.p_inf()};
+}
 }  // namespace material
 
 // ---- limiters (limiting/) -----------------------------------------------------
@@ -241,8 +262,9 @@ struct SplitSolver {
              double* max_ws_out = nullptr) const {
     void* pin = in.data();
     void* pout = out.data();
-    check(fl_split_solve(&in.grid(), &pin, &pout, (double)mat.adiabatic(), (double)dtdh,
-                         policy, setter.mask, max_ws_out, stream));
+    const fl_material m = material::to_fl(mat);
+    check(fl_split_solve_mat(&in.grid(), &pin, &pout, &m, (double)dtdh, policy, setter.mask,
+                             max_ws_out, stream));
     if (pout != out.data()) in.swap(out);
   }
 };
@@ -316,16 +338,18 @@ class SimulatorImpl {
     const int64_t cells = g.n[0] * g.n[1] * g.n[2];
     std::vector<T> host((dimensions + 2) * (std::size_t)g.pitch);
     const T gm = mat_.adiabatic();
+    const T pinf = mat_.p_inf();
     float pos[3] = {0.f, 0.f, 0.f};
     for (int64_t i = 0; i < cells; ++i) {
       const int64_t c[3] = {i % g.n[0], (i / g.n[0]) % g.n[1], i / (g.n[0] * g.n[1])};
       for (std::size_t d = 0; d < dimensions; ++d) pos[d] = float(c[d]) / float(g.n[d]);
       T prim[5];
       for (std::size_t k = 0; k < dimensions + 2; ++k) prim[k] = (T)fillers[k].filler(pos);
-      // primitive -> conservative (state_impl.hpp:390-406)
+      // primitive -> conservative (state_impl.hpp:390-406), e from the eos
+      // (ideal_gas.hpp:59-63; stiff_fluid.hpp:76-80)
       T v2 = T(0);
       for (std::size_t d = 0; d < dimensions; ++d) v2 += prim[2 + d] * prim[2 + d];
-      const T e = prim[1] / ((gm - T(1)) * prim[0]);
+      const T e = (prim[1] + gm * pinf) / ((gm - T(1)) * prim[0]);
       host[0 * g.pitch + i] = prim[0];
       host[1 * g.pitch + i] = prim[0] * (T(0.5) * v2 + e);
       for (std::size_t d = 0; d < dimensions; ++d) host[(2 + d) * g.pitch + i] = prim[2 + d] * prim[0];
@@ -343,6 +367,8 @@ class SimulatorImpl {
       fl_grid g = grid();
       check(fl_sim_create(&sim_, &g, (double)mat_.adiabatic(), policy, setter_.mask));
     }
+    const fl_material m = material::to_fl(mat_);
+    check(fl_sim_set_material(sim_, &m));
     void* res = nullptr;
     check(fl_simulate(sim_, a_.data(), b_.data(), cfl_, res_, sim_time_, max_iters_, stream,
                       &iters_, &run_time_, &res));

@@ -54,7 +54,11 @@ static double pressure2(const double* u, double g) {
   return (g - 1.0) * (u[1] - 0.5 * r * (vx * vx + vy * vy));
 }
 
-static double sound2(const double* u, double g) { return sqrt(g * pressure2(u, g) / u[0]); }
+/* sound speed with the material's p_inf (stiff_fluid.hpp:92-96; 0 for the
+ * ideal gas, ideal_gas.hpp:75-78: p + 0 = p) */
+static double sound2(const double* u, double g, double pinf) {
+  return sqrt(g * (pressure2(u, g) + pinf) / u[0]);
+}
 
 /* Hllc::wavespeed_slr (flux_method/flux_hllc.hpp:447-462) */
 static double wavespeed_slr(const double* u, double pstar, double a, double q, double g) {
@@ -67,8 +71,9 @@ static double wavespeed_slr(const double* u, double pstar, double a, double q, d
 /* Hllc::solve_star_conservative_left (flux_method/flux_hllc.hpp:330-361)
  * with q_k (:425-430), wavespeed_star (:490-513) and star_state_cons
  * (:532-568), normal direction x. */
-static void star_left(const double* ul, const double* ur, double gl, double gr, double* out) {
-  const double al = sound2(ul, gl), ar = sound2(ur, gr);
+static void star_left(const double* ul, const double* ur, double gl, double gr, double il,
+                      double ir, double* out) {
+  const double al = sound2(ul, gl, il), ar = sound2(ur, gr, ir);
   const double pl = pressure2(ul, gl), pr = pressure2(ur, gr);
   const double vl = ul[2] / ul[0], vr = ur[2] / ur[0];
   const double p_pvrs = 0.5 * ((pl + pr) - (0.25 * (vr - vl) * (ur[0] + ul[0]) * (al + ar)));
@@ -83,6 +88,12 @@ static void star_left(const double* ul, const double* ur, double gl, double gr, 
   for (int c = 0; c < 4; ++c) out[c] = scale * ul[c];
   out[2] = s_star * ul[0] * scale;
   out[1] = scale * (ul[1] + ul[0] * (s_star - vl) * (s_star + pl / (ul[0] * sf)));
+}
+
+/* star_left for the pin against the reference's function */
+void flo_mm_star_left(const double* ul, const double* ur, double gl, double il, double gr,
+                      double ir, double* out) {
+  star_left(ul, ur, gl, gr, il, ir, out);
 }
 
 static void load4(const double* u, int64_t pitch, int64_t i, double* o) {
@@ -140,7 +151,7 @@ static int gfm_source(const double* pa, const double* pb, int64_t nx, int64_t ny
 /* star state of source (x, y) of material A (riemann_ghost_fluid.hpp:70-176) */
 static void gfm_star(const double* ua, const double* ub, int64_t pitch, int64_t nx, int64_t ny,
                      const double* pa, int64_t x, int64_t y, double h, const double* n, double ga,
-                     double gb, double* star) {
+                     double gb, double ia, double ib, double* star) {
   const double abs_phi = fabs(pa[y * nx + x]);
   const double h32 = 1.5 * h;
   double w[2], wl[4], wr[4];
@@ -158,7 +169,7 @@ static void gfm_star(const double* ua, const double* ub, int64_t pitch, int64_t 
   wr[2] = vr_n * wr[0];
   wl[3] = 0.0 * wl[0];
   wr[3] = 0.0 * wr[0];
-  star_left(wl, wr, ga, gb, star);
+  star_left(wl, wr, ga, gb, ia, ib, star);
   /* rotate back, dimension by dimension on the updated star state */
   for (int d = 0; d < 2; ++d) {
     const double sv = star[2 + d] / star[0];
@@ -169,8 +180,9 @@ static void gfm_star(const double* ua, const double* ub, int64_t pitch, int64_t 
 
 /* GFM for both materials from the pre-pass states; u0/u1 updated in place.
  * Returns the number of target cells written. */
-int64_t flo_mm_gfm(int64_t nx, int64_t ny, int64_t pitch, double h, double g0, double g1,
-                   double* u0, double* u1, const double* p0, const double* p1, int f32) {
+int64_t flo_mm_gfm_mat(int64_t nx, int64_t ny, int64_t pitch, double h, double g0, double i0,
+                       double g1, double i1, double* u0, double* u1, const double* p0,
+                       const double* p1, int f32) {
   const int64_t n = nx * ny;
   double* snap0 = (double*)malloc(sizeof(double) * 4 * pitch);
   double* snap1 = (double*)malloc(sizeof(double) * 4 * pitch);
@@ -184,13 +196,14 @@ int64_t flo_mm_gfm(int64_t nx, int64_t ny, int64_t pitch, double h, double g0, d
     const double* ub = m == 0 ? snap1 : snap0;
     double* dst = m == 0 ? u0 : u1;
     const double ga = m == 0 ? g0 : g1, gb = m == 0 ? g1 : g0;
+    const double ia = m == 0 ? i0 : i1, ib = m == 0 ? i1 : i0;
     for (int64_t y = 0; y < ny; ++y)
       for (int64_t x = 0; x < nx; ++x) {
         double nrm[2], star[4];
         if (!gfm_source(pa, pb, nx, ny, x, y, h, nrm)) continue;
         const int64_t tx = x + isgn(nrm[0]), ty = y + isgn(nrm[1]);
         if (tx < 0 || tx >= nx || ty < 0 || ty >= ny) continue;
-        gfm_star(ua, ub, pitch, nx, ny, pa, x, y, h, nrm, ga, gb, star);
+        gfm_star(ua, ub, pitch, nx, ny, pa, x, y, h, nrm, ga, gb, ia, ib, star);
         const int64_t t = ty * nx + tx;
         for (int c = 0; c < 4; ++c) dst[c * pitch + t] = st(star[c], f32);
         ++written;
@@ -200,6 +213,11 @@ int64_t flo_mm_gfm(int64_t nx, int64_t ny, int64_t pitch, double h, double g0, d
   free(snap1);
   (void)n;
   return written;
+}
+
+int64_t flo_mm_gfm(int64_t nx, int64_t ny, int64_t pitch, double h, double g0, double g1,
+                   double* u0, double* u1, const double* p0, const double* p1, int f32) {
+  return flo_mm_gfm_mat(nx, ny, pitch, h, g0, 0.0, g1, 0.0, u0, u1, p0, p1, f32);
 }
 
 /* band of the extrapolation: dh <= phi <= 6 dh / sqrt(2), phi > 0
@@ -281,17 +299,18 @@ int flo_mm_extrapolate(int64_t nx, int64_t ny, int64_t pitch, double h, double* 
 
 /* set_states (state/cuda/state_initialization.cuh:72-86): cells inside the
  * level set (phi <= 0) take the conservative form of prim (rho, p, vx, vy). */
-void flo_mm_set_states(int64_t n, int64_t pitch, double* u, const double* phi, const double* prim,
-                       double g, int f32) {
+void flo_mm_set_states_mat(int64_t n, int64_t pitch, double* u, const double* phi,
+                           const double* prim, double g, double pinf, int f32) {
   /* prim -> cons in the state's precision (state/state_impl.hpp:390-406) */
   double cons[4];
   if (f32) {
     const float r = (float)prim[0], p = (float)prim[1], vx = (float)prim[2], vy = (float)prim[3];
-    const float gf = (float)g;
+    const float gf = (float)g, pf = (float)pinf;
     float v2 = 0.0f;
     v2 += vx * vx;
     v2 += vy * vy;
-    const float e = p / ((gf - 1.0f) * r);
+    /* e from the eos (ideal_gas.hpp:59-63; stiff_fluid.hpp:76-80) */
+    const float e = (p + gf * pf) / ((gf - 1.0f) * r);
     cons[0] = r;
     cons[1] = r * (0.5f * v2 + e);
     cons[2] = vx * r;
@@ -301,7 +320,7 @@ void flo_mm_set_states(int64_t n, int64_t pitch, double* u, const double* phi, c
     double v2 = 0.0;
     v2 += vx * vx;
     v2 += vy * vy;
-    const double e = p / ((g - 1.0) * r);
+    const double e = (p + g * pinf) / ((g - 1.0) * r);
     cons[0] = r;
     cons[1] = r * (0.5 * v2 + e);
     cons[2] = vx * r;
@@ -311,6 +330,11 @@ void flo_mm_set_states(int64_t n, int64_t pitch, double* u, const double* phi, c
     if (!(phi[i] <= 0.0 || phi[i] <= -0.0)) continue;
     for (int c = 0; c < 4; ++c) u[c * pitch + i] = cons[c];
   }
+}
+
+void flo_mm_set_states(int64_t n, int64_t pitch, double* u, const double* phi, const double* prim,
+                       double g, int f32) {
+  flo_mm_set_states_mat(n, pitch, u, phi, prim, g, 0.0, f32);
 }
 
 /* combine_into_first (material/cuda/combine_materials.cuh:39-66): cells

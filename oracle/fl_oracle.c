@@ -13,6 +13,14 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* The stiffened fluid's material constant (material/stiff_fluid.hpp:38-133);
+ * 0 is the ideal gas.  One value for the whole library: the oracle runs one
+ * material at a time (flo_set_p_inf). */
+static double flo_p_inf_ = 0.0;
+
+void flo_set_p_inf(double p_inf) { flo_p_inf_ = p_inf; }
+double flo_get_p_inf(void) { return flo_p_inf_; }
+
 #define T double
 #define SFX _f64
 #define SQRT(x) sqrt(x)

@@ -49,6 +49,13 @@ typedef struct flo_policy {
   uint32_t reflect;   /* bit d set: dimension d has reflective ends */
 } flo_policy;
 
+/* Material: p_inf = 0 (the default) is the ideal gas; p_inf > 0 the
+ * stiffened fluid (material/stiff_fluid.hpp:38-133), which changes the sound
+ * speed and the energy of prim_to_cons / fill_riemann.  Applies to every
+ * call that follows. */
+void flo_set_p_inf(double p_inf);
+double flo_get_p_inf(void);
+
 /* One dimensional sweep: out = in + dtdh * (F(i-1/2) - F(i+1/2)) along dim. */
 int flo_sweep_f64(const flo_grid* g, int dim, const double* in, double* out,
                   double gamma, double dtdh, const flo_policy* pol);

@@ -14,6 +14,7 @@ planes ``[rho, E, m_x, m_y, m_z]``, x fastest) unless noted.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -97,12 +98,22 @@ def lib():
                                  C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_int]
         L.flo_mm_gfm.restype = C.c_int64
+        L.flo_mm_gfm_mat.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.flo_mm_gfm_mat.restype = C.c_int64
         L.flo_mm_extrapolate.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_void_p,
                                          C.c_void_p, C.c_int, C.c_int]
         L.flo_mm_extrapolate.restype = C.c_int
         L.flo_mm_set_states.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_double, C.c_int]
+        L.flo_mm_star_left.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_void_p]
+        L.flo_mm_set_states_mat.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_double, C.c_double, C.c_int]
         L.flo_mm_combine.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.flo_set_p_inf.argtypes = [C.c_double]
+        L.flo_get_p_inf.restype = C.c_double
         _lib = L
     return _lib
 
@@ -127,8 +138,28 @@ def ref():
                                        C.c_double, C.c_int64, C.c_int, C.c_int, C.c_int,
                                        C.c_uint32, P(C.c_int), P(C.c_double), C.c_void_p, C.c_int64]
         L.ref_simulate_f64.restype = C.c_int64
+        L.ref_set_p_inf.argtypes = [C.c_double]
+        L.ref_star_left_2d.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_void_p]
+        L.ref_prim_to_cons_f64.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p]
         _ref = L
     return _ref
+
+
+@contextlib.contextmanager
+def stiffened(p_inf: float):
+    """Within the block, the oracle (and the reference-functor build, when
+    present) compute for the stiffened fluid with this p_inf
+    (material/stiff_fluid.hpp:38-133) instead of the ideal gas."""
+    lib().flo_set_p_inf(float(p_inf))
+    if ref_available():
+        ref().ref_set_p_inf(float(p_inf))
+    try:
+        yield
+    finally:
+        lib().flo_set_p_inf(0.0)
+        if ref_available():
+            ref().ref_set_p_inf(0.0)
 
 
 def _grid(shape) -> _Grid:
@@ -290,6 +321,32 @@ def ref_sweep(shape, dim, u, gamma, dtdh, flux="hllc", limiter="vanleer",
     return out
 
 
+def ref_prim_to_cons(prim, gamma):
+    """The reference's State::conservative of one primitive state (FP64)."""
+    prim = np.ascontiguousarray(prim, dtype=np.float64)
+    out = np.empty_like(prim)
+    ref().ref_prim_to_cons_f64(prim.shape[0] - 2, _ptr(prim), gamma, _ptr(out))
+    return out
+
+
+def mm_star_left(ul, ur, gl, il, gr, ir):
+    """The oracle's two-material HLLC star state (left side, normal x)."""
+    ul = np.ascontiguousarray(ul, dtype=np.float64)
+    ur = np.ascontiguousarray(ur, dtype=np.float64)
+    out = np.empty(4)
+    lib().flo_mm_star_left(_ptr(ul), _ptr(ur), gl, il, gr, ir, _ptr(out))
+    return out
+
+
+def ref_star_left(ul, ur, gl, il, gr, ir):
+    """The reference's Hllc::solve_star_conservative_left, 2-D states."""
+    ul = np.ascontiguousarray(ul, dtype=np.float64)
+    ur = np.ascontiguousarray(ur, dtype=np.float64)
+    out = np.empty(4)
+    ref().ref_star_left_2d(_ptr(ul), _ptr(ur), gl, il, gr, ir, _ptr(out))
+    return out
+
+
 def ref_max_wavespeed(shape, u, gamma):
     D = len(shape)
     n = (C.c_int64 * 3)(*(list(shape) + [1] * (3 - D)))
@@ -360,14 +417,15 @@ def _as_f64(u):
     return np.ascontiguousarray(u, dtype=np.float64).copy()
 
 
-def mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1):
-    """Riemann ghost-fluid star states for both materials; returns (u0, u1, n)."""
+def mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1, p_infs=(0.0, 0.0)):
+    """Riemann ghost-fluid star states for both materials; returns (u0, u1, n).
+    p_infs: each material's stiffened-fluid constant (0: ideal gas)."""
     f32 = u0.dtype == np.float32
     a, b = _as_f64(u0), _as_f64(u1)
     p0 = np.ascontiguousarray(phi0, dtype=np.float64)
     p1 = np.ascontiguousarray(phi1, dtype=np.float64)
-    n = lib().flo_mm_gfm(nx, ny, a.shape[1], h, gammas[0], gammas[1], _ptr(a), _ptr(b), _ptr(p0),
-                         _ptr(p1), int(f32))
+    n = lib().flo_mm_gfm_mat(nx, ny, a.shape[1], h, gammas[0], p_infs[0], gammas[1], p_infs[1],
+                             _ptr(a), _ptr(b), _ptr(p0), _ptr(p1), int(f32))
     dt = np.float32 if f32 else np.float64
     return a.astype(dt), b.astype(dt), int(n)
 
@@ -381,20 +439,21 @@ def mm_extrapolate(nx, ny, h, u, phi, max_iters=64):
     return a.astype(u.dtype), int(it)
 
 
-def mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters=64):
+def mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters=64, p_infs=(0.0, 0.0)):
     """GFM for both materials, then the extrapolation of each."""
-    u0, u1, _ = mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1)
+    u0, u1, _ = mm_gfm(nx, ny, h, gammas, u0, u1, phi0, phi1, p_infs)
     u0, _ = mm_extrapolate(nx, ny, h, u0, phi0, max_iters)
     u1, _ = mm_extrapolate(nx, ny, h, u1, phi1, max_iters)
     return u0, u1
 
 
-def mm_set_states(u, phi, prim, gamma):
+def mm_set_states(u, phi, prim, gamma, p_inf=0.0):
     f32 = u.dtype == np.float32
     a = _as_f64(u)
     p = np.ascontiguousarray(phi, dtype=np.float64)
     pr = np.ascontiguousarray(prim, dtype=np.float64)
-    lib().flo_mm_set_states(p.size, a.shape[1], _ptr(a), _ptr(p), _ptr(pr), gamma, int(f32))
+    lib().flo_mm_set_states_mat(p.size, a.shape[1], _ptr(a), _ptr(p), _ptr(pr), gamma, p_inf,
+                                int(f32))
     return a.astype(u.dtype)
 
 
@@ -406,21 +465,26 @@ def mm_combine(u0, u1, phi1):
     return a.astype(u0.dtype)
 
 
-def mm_step(nx, ny, h, gammas, cfl, u0, u1, phi0, phi1, reinit, max_iters=64):
+def mm_step(nx, ny, h, gammas, cfl, u0, u1, phi0, phi1, reinit, max_iters=64,
+            p_infs=(0.0, 0.0)):
     """One step of the two-material loop: ghost cells, CFL time step over
     both materials, split MUSCL-Hancock/HLLC step of each material with its
-    own gamma, level-set velocity, RK3 advection, projection and (when
-    reinit) reinitialisation of both level sets.  Returns
+    own equation of state, level-set velocity, RK3 advection, projection and
+    (when reinit) reinitialisation of both level sets.  Returns
     (u0, u1, phi0, phi1, dt)."""
     shape = (nx, ny)
-    u0, u1 = mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters)
-    ws = max(float(max_wavespeed(shape, u0, gammas[0])), float(max_wavespeed(shape, u1, gammas[1])))
-    dt = cfl * h / ws
+    u0, u1 = mm_ghost(nx, ny, h, gammas, u0, u1, phi0, phi1, max_iters, p_infs)
+    ws = []
+    for u, g, pi in ((u0, gammas[0], p_infs[0]), (u1, gammas[1], p_infs[1])):
+        with stiffened(pi):
+            ws.append(float(max_wavespeed(shape, u, g)))
+    dt = cfl * h / max(ws)
     dtdh = dt / h
     out = []
-    for u, g in ((u0, gammas[0]), (u1, gammas[1])):
-        v = sweep(shape, 0, u, g, dtdh)
-        v = sweep(shape, 1, v, g, dtdh)
+    for u, g, pi in ((u0, gammas[0], p_infs[0]), (u1, gammas[1], p_infs[1])):
+        with stiffened(pi):
+            v = sweep(shape, 0, u, g, dtdh)
+            v = sweep(shape, 1, v, g, dtdh)
         out.append(v)
     u0, u1 = out
     vel = ls_velocity(nx, ny, [phi0, phi1], [u0.astype(np.float64), u1.astype(np.float64)], h)

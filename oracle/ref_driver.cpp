@@ -32,6 +32,7 @@
 #include <fluidity/limiting/superbee_limiter.hpp>
 #include <fluidity/limiting/van_leer_limiter.hpp>
 #include <fluidity/material/ideal_gas.hpp>
+#include <fluidity/material/stiff_fluid.hpp>
 #include <fluidity/reconstruction/basic_reconstructor.hpp>
 #include <fluidity/reconstruction/muscl_reconstructor.hpp>
 #include <fluidity/simulator/parameters.hpp>
@@ -45,8 +46,17 @@
 
 namespace {
 
-using mat_t = fluid::material::IdealGas<double>;
+using ideal_t = fluid::material::IdealGas<double>;
+using stiff_t = fluid::material::StiffFluid<double>;
 using form_t = fluid::limit::cons_form_t;
+
+// The material of the calls that follow: the ideal gas while p_inf is 0, else
+// the reference's StiffFluid(gamma, p_inf).
+double g_p_inf = 0.0;
+
+template <typename Mat> Mat make_mat(double gamma);
+template <> ideal_t make_mat<ideal_t>(double gamma) { return ideal_t(gamma); }
+template <> stiff_t make_mat<stiff_t>(double gamma) { return stiff_t(gamma, g_p_inf); }
 constexpr int kPad = 4;
 
 template <int D>
@@ -140,15 +150,15 @@ void load_padded(const Grid& g, const double* in, uint32_t reflect, Padded<D>& p
 
 // One sweep: out = U + dtdh * FaceFlux::flux_delta(U, dim)
 // (split_solver.hpp:160).
-template <int D, typename Recon, typename Flux, int Dim>
+template <int D, typename Mat, typename Recon, typename Flux, int Dim>
 void sweep_t(const Grid& g, const double* in, double* out, double gamma,
              double dtdh, uint32_t reflect) {
-  using ff_t = fluid::solver::FaceFlux<Recon, Flux, mat_t>;
+  using ff_t = fluid::solver::FaceFlux<Recon, Flux, Mat>;
   using it_t = fluid::MultidimIterator<state_t<D>, fluid::DimInfo<D>, fluid::exec::cpu_t>;
   Padded<D> p(g);
   load_padded<D>(g, in, reflect, p);
   const auto info = make_info<D>(p.np);
-  const ff_t ff(mat_t(gamma), dtdh);
+  const ff_t ff(make_mat<Mat>(gamma), dtdh);
 #pragma omp parallel for collapse(2) schedule(static)
   for (int64_t z = 0; z < p.n[2]; ++z)
     for (int64_t y = 0; y < p.n[1]; ++y)
@@ -160,37 +170,46 @@ void sweep_t(const Grid& g, const double* in, double* out, double gamma,
       }
 }
 
-template <int D, typename Recon, typename Flux>
+template <int D, typename Mat, typename Recon, typename Flux>
 void sweep_dim(const Grid& g, int dim, const double* in, double* out, double gamma,
                double dtdh, uint32_t reflect) {
-  if (dim == 0) sweep_t<D, Recon, Flux, 0>(g, in, out, gamma, dtdh, reflect);
-  if constexpr (D > 1) if (dim == 1) sweep_t<D, Recon, Flux, 1>(g, in, out, gamma, dtdh, reflect);
-  if constexpr (D > 2) if (dim == 2) sweep_t<D, Recon, Flux, 2>(g, in, out, gamma, dtdh, reflect);
+  if (dim == 0) sweep_t<D, Mat, Recon, Flux, 0>(g, in, out, gamma, dtdh, reflect);
+  if constexpr (D > 1) if (dim == 1) sweep_t<D, Mat, Recon, Flux, 1>(g, in, out, gamma, dtdh, reflect);
+  if constexpr (D > 2) if (dim == 2) sweep_t<D, Mat, Recon, Flux, 2>(g, in, out, gamma, dtdh, reflect);
 }
 
-template <int D, typename Recon>
+template <int D, typename Mat, typename Recon>
 int sweep_flux(const Grid& g, int dim, const double* in, double* out, double gamma,
                double dtdh, int flux, uint32_t reflect) {
+  using namespace fluid::flux;
   switch (flux) {
-    case 0: sweep_dim<D, Recon, fluid::flux::Hllc>(g, dim, in, out, gamma, dtdh, reflect); return 0;
-    case 1: sweep_dim<D, Recon, fluid::flux::Force>(g, dim, in, out, gamma, dtdh, reflect); return 0;
-    case 2: sweep_dim<D, Recon, fluid::flux::LaxFriedrichs>(g, dim, in, out, gamma, dtdh, reflect); return 0;
-    case 3: sweep_dim<D, Recon, fluid::flux::Richtmyer>(g, dim, in, out, gamma, dtdh, reflect); return 0;
+    case 0: sweep_dim<D, Mat, Recon, Hllc>(g, dim, in, out, gamma, dtdh, reflect); return 0;
+    case 1: sweep_dim<D, Mat, Recon, Force>(g, dim, in, out, gamma, dtdh, reflect); return 0;
+    case 2: sweep_dim<D, Mat, Recon, LaxFriedrichs>(g, dim, in, out, gamma, dtdh, reflect); return 0;
+    case 3: sweep_dim<D, Mat, Recon, Richtmyer>(g, dim, in, out, gamma, dtdh, reflect); return 0;
   }
   return -1;
+}
+
+template <int D, typename Mat>
+int sweep_recon(const Grid& g, int dim, const double* in, double* out, double gamma,
+                double dtdh, int flux, int limiter, int recon, uint32_t reflect) {
+  if (recon == 1)
+    return sweep_flux<D, Mat, fluid::recon::BasicReconstructor<fluid::limit::VanLeer<form_t>>>(
+        g, dim, in, out, gamma, dtdh, flux, reflect);
+  if (limiter == 1)
+    return sweep_flux<D, Mat, fluid::recon::MHReconstructor<fluid::limit::Superbee<form_t>>>(
+        g, dim, in, out, gamma, dtdh, flux, reflect);
+  return sweep_flux<D, Mat, fluid::recon::MHReconstructor<fluid::limit::VanLeer<form_t>>>(
+      g, dim, in, out, gamma, dtdh, flux, reflect);
 }
 
 template <int D>
 int sweep_all(const Grid& g, int dim, const double* in, double* out, double gamma,
               double dtdh, int flux, int limiter, int recon, uint32_t reflect) {
-  if (recon == 1)
-    return sweep_flux<D, fluid::recon::BasicReconstructor<fluid::limit::VanLeer<form_t>>>(
-        g, dim, in, out, gamma, dtdh, flux, reflect);
-  if (limiter == 1)
-    return sweep_flux<D, fluid::recon::MHReconstructor<fluid::limit::Superbee<form_t>>>(
-        g, dim, in, out, gamma, dtdh, flux, reflect);
-  return sweep_flux<D, fluid::recon::MHReconstructor<fluid::limit::VanLeer<form_t>>>(
-      g, dim, in, out, gamma, dtdh, flux, reflect);
+  if (g_p_inf != 0.0)
+    return sweep_recon<D, stiff_t>(g, dim, in, out, gamma, dtdh, flux, limiter, recon, reflect);
+  return sweep_recon<D, ideal_t>(g, dim, in, out, gamma, dtdh, flux, limiter, recon, reflect);
 }
 
 bool valid(const Grid& g) {
@@ -203,9 +222,9 @@ bool valid(const Grid& g) {
   return g.pitch >= cells;
 }
 
-template <int D>
+template <int D, typename Mat>
 double max_ws(const Grid& g, const double* in, double gamma) {
-  const mat_t mat(gamma);
+  const Mat mat = make_mat<Mat>(gamma);
   int64_t cells = 1;
   for (int d = 0; d < D; ++d) cells *= g.n[d];
   double m = 0.0;
@@ -241,12 +260,58 @@ int ref_sweep_f64(int dims, const int64_t* n, int64_t pitch, int dim,
 double ref_max_wavespeed_f64(int dims, const int64_t* n, int64_t pitch,
                              const double* in, double gamma) {
   const Grid g{dims, {n[0], dims > 1 ? n[1] : 1, dims > 2 ? n[2] : 1}, pitch};
+  const bool stiff = g_p_inf != 0.0;
   switch (dims) {
-    case 1: return max_ws<1>(g, in, gamma);
-    case 2: return max_ws<2>(g, in, gamma);
-    case 3: return max_ws<3>(g, in, gamma);
+    case 1: return stiff ? max_ws<1, stiff_t>(g, in, gamma) : max_ws<1, ideal_t>(g, in, gamma);
+    case 2: return stiff ? max_ws<2, stiff_t>(g, in, gamma) : max_ws<2, ideal_t>(g, in, gamma);
+    case 3: return stiff ? max_ws<3, stiff_t>(g, in, gamma) : max_ws<3, ideal_t>(g, in, gamma);
   }
   return -1.0;
+}
+
+void ref_set_p_inf(double p_inf) { g_p_inf = p_inf; }
+
+// Hllc::solve_star_conservative_left (flux_method/flux_hllc.hpp:330-361) for
+// 2-D conservative states of two materials, normal direction x; a material
+// is the ideal gas when its p_inf is 0, else StiffFluid(gamma, p_inf).
+void ref_star_left_2d(const double* ul, const double* ur, double gl, double il, double gr,
+                      double ir, double* out) {
+  using st_t = state_t<2>;
+  st_t l, r;
+  for (int k = 0; k < 4; ++k) {
+    l[k] = ul[k];
+    r[k] = ur[k];
+  }
+  auto run = [&](const auto& eosl, const auto& eosr) {
+    const st_t s = fluid::flux::Hllc::solve_star_conservative_left(l, r, eosl, eosr,
+                                                                  fluid::dimx_t());
+    for (int k = 0; k < 4; ++k) out[k] = s[k];
+  };
+  if (il == 0.0 && ir == 0.0) run(ideal_t(gl), ideal_t(gr));
+  else if (il == 0.0) run(ideal_t(gl), stiff_t(gr, ir));
+  else if (ir == 0.0) run(stiff_t(gl, il), ideal_t(gr));
+  else run(stiff_t(gl, il), stiff_t(gr, ir));
+}
+
+// Primitive -> conservative with the reference's State::conservative
+// (state/state_impl.hpp:390-406) and the current material's eos.
+void ref_prim_to_cons_f64(int dims, const double* prim, double gamma, double* cons) {
+  auto run = [&](auto dim_tag, auto mat) {
+    constexpr int D = decltype(dim_tag)::value;
+    fluid::state::primitive_t<double, D> s;
+    for (int k = 0; k < D + 2; ++k) s[k] = prim[k];
+    const auto c = s.conservative(mat);
+    for (int k = 0; k < D + 2; ++k) cons[k] = c[k];
+  };
+  const bool stiff = g_p_inf != 0.0;
+  switch (dims) {
+    case 1: stiff ? run(std::integral_constant<int, 1>{}, make_mat<stiff_t>(gamma))
+                  : run(std::integral_constant<int, 1>{}, make_mat<ideal_t>(gamma)); break;
+    case 2: stiff ? run(std::integral_constant<int, 2>{}, make_mat<stiff_t>(gamma))
+                  : run(std::integral_constant<int, 2>{}, make_mat<ideal_t>(gamma)); break;
+    default: stiff ? run(std::integral_constant<int, 3>{}, make_mat<stiff_t>(gamma))
+                   : run(std::integral_constant<int, 3>{}, make_mat<ideal_t>(gamma)); break;
+  }
 }
 
 // SimulatorImpl::simulate's loop with the reference's own Parameters.

@@ -8,7 +8,9 @@ oracle/_ref/libfluidity_ref.so and driven by oracle/ref_driver.cpp.  Inputs
 are seeded.  Run from the repository root (needs the reference tree to build
 the library):
 
-    python oracle/build_ref.sh && python tests/golden/make_golden.py
+    bash oracle/build_ref.sh && python tests/golden/make_golden.py
+
+stiff.npz holds the same kinds of cases for the stiffened fluid.
 """
 import os
 import sys
@@ -90,6 +92,75 @@ def simulate_cases():
     return cases
 
 
+# Stiffened fluid (material/stiff_fluid.hpp:38-133): the reference's
+# StiffFluid(gamma, p_inf) in place of IdealGas; (4.4, 0.613) is the water of
+# the reference's gas-water validation (StiffFluid{4.4} keeps p_inf = 0.613).
+STIFF = [(4.4, 0.613), (6.12, 343.0)]
+
+
+def stiff_cases():
+    cases = {}
+    specs = [("rand1d_64", (64,), 0), ("smooth2d_32x16", (32, 16), 3),
+             ("rand3d_10x8x6", (10, 8, 6), 5)]
+    pols = [("hllc", "vanleer", "muscl"), ("force", "superbee", "muscl"),
+            ("lf", "vanleer", "basic"), ("richtmyer", "vanleer", "muscl")]
+    for k, (gamma, p_inf) in enumerate(STIFF):
+        with O.stiffened(p_inf):
+            for seed, (name, shape, refl) in enumerate(specs):
+                smooth = name.startswith("smooth")
+                prim = random_prim(shape, 300 + 10 * k + seed, smooth=smooth, mild=True)
+                u = np.stack([O.ref_prim_to_cons(prim[:, i], gamma)
+                              for i in range(prim.shape[1])], axis=1)
+                ws = O.ref_max_wavespeed(shape, u, gamma)
+                dtdh = 0.8 / ws
+                tag = f"g{k}_{name}"
+                cases[f"{tag}__maxws"] = dict(shape=np.array(shape), u=u, ws=ws, gamma=gamma,
+                                              p_inf=p_inf, prim=prim)
+                for flux, lim, recon in pols:
+                    for dim in range(len(shape)):
+                        out = O.ref_sweep(shape, dim, u, gamma, dtdh, flux=flux, limiter=lim,
+                                          recon=recon, reflect=refl)
+                        # input: the u of case "<tag>__maxws"
+                        cases[f"{tag}__{flux}_{lim}_{recon}_d{dim}"] = dict(
+                            shape=np.array(shape), dim=dim, src=tag, out=out, dtdh=dtdh,
+                            flux=flux, limiter=lim, recon=recon, reflect=refl, gamma=gamma,
+                            p_inf=p_inf)
+            # whole runs: a 1-D tube and 2-D quadrants, filled as fill_data does
+            for name, shape, dims_seed, cfl, steps, flux in (
+                    ("tube1d_200", (200,), 31, 0.9, 40, "hllc"),
+                    ("quad2d_40x32", (40, 32), 32, 0.8, 6, "force")):
+                D = len(shape)
+                st = riemann_states(dims_seed, D)
+                u = O.fill_riemann(shape, st, gamma)
+                for i in range(2 ** D):       # the oracle's fill against the reference's
+                    ref_c = O.ref_prim_to_cons(st[i], gamma)
+                    assert np.array_equal(O.prim_to_cons(st[i], gamma), ref_c)
+                out, n, rt, dts = O.ref_simulate(shape, u, gamma, cfl, 1.0 / shape[0], 1e30,
+                                                 steps, flux=flux)
+                cases[f"g{k}_{name}_{flux}"] = dict(
+                    shape=np.array(shape), states=st, u=u, out=out, steps=n, run_time=rt,
+                    dts=dts, cfl=cfl, res=1.0 / shape[0], sim_time=1e30, max_iters=steps,
+                    flux=flux, limiter="vanleer", recon="muscl", reflect=0, gamma=gamma,
+                    p_inf=p_inf)
+    # the two-material HLLC star state (Hllc::solve_star_conservative_left,
+    # flux_hllc.hpp:330-361) for every pairing of ideal gas and stiffened fluid
+    rng = np.random.default_rng(77)
+    for k in range(64):
+        gl, gr = rng.uniform(1.1, 6.0, 2)
+        il = 0.0 if k % 4 in (0, 1) else float(rng.uniform(0.0, 50.0))
+        ir = 0.0 if k % 4 in (0, 2) else float(rng.uniform(0.0, 50.0))
+        sides = []
+        for g, pi in ((gl, il), (gr, ir)):
+            prim = np.array([rng.uniform(0.5, 3.0), rng.uniform(0.5, 20.0),
+                             rng.uniform(-2.0, 2.0), rng.uniform(-2.0, 2.0)])
+            with O.stiffened(pi):
+                sides.append(O.ref_prim_to_cons(prim, g))
+        star = O.ref_star_left(sides[0], sides[1], gl, il, gr, ir)
+        cases[f"star_{k:02d}"] = dict(ul=sides[0], ur=sides[1], gl=gl, il=il, gr=gr, ir=ir,
+                                      star=star)
+    return cases
+
+
 def check_finite(cases):
     # multi-step cases must stay finite: a blown-up state (NaN) is flagged as
     # an error by the GPU path, while the reference's max_element silently
@@ -124,5 +195,8 @@ if __name__ == "__main__":
     sims = simulate_cases()
     check_finite(sims)
     save("simulate.npz", sims)
-    for f in ("sweeps.npz", "simulate.npz"):
+    stiff = stiff_cases()
+    check_finite({k: v for k, v in stiff.items() if "out" in v and "dim" not in v})
+    save("stiff.npz", stiff)
+    for f in ("sweeps.npz", "simulate.npz", "stiff.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")

@@ -11,11 +11,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
-def compile_program(tmp_path):
+def compile_program(tmp_path, name="toro_case1"):
     from fluidity_b200 import build
     lib = build.build()
-    exe = str(tmp_path / "toro_case1")
-    cmd = ["g++", "-O2", "-std=c++17", os.path.join(ROOT, "tests", "cpp", "toro_case1.cpp"),
+    exe = str(tmp_path / name)
+    cmd = ["g++", "-O2", "-std=c++17", os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
            f"-I{os.path.join(ROOT, 'include')}", f"-I{CUDA}/include",
            f"-L{os.path.dirname(lib)}", "-lfluidity_b200", f"-L{CUDA}/lib64", "-lcudart",
            f"-Wl,-rpath,{os.path.dirname(lib)}", "-o", exe]
@@ -23,8 +23,9 @@ def compile_program(tmp_path):
     return exe
 
 
-def test_cpp_interface_compiles(tmp_path):
-    assert os.path.exists(compile_program(tmp_path))
+@pytest.mark.parametrize("name", ["toro_case1", "stiff_tube"])
+def test_cpp_interface_compiles(tmp_path, name):
+    assert os.path.exists(compile_program(tmp_path, name))
 
 
 @pytest.mark.gpu
@@ -51,3 +52,22 @@ def test_cpp_toro_case1_matches_oracle(cuda, oracle, tmp_path):
         vals = np.array([float(t) for t in text.split()])
         assert vals.shape == (n,)
         assert np.allclose(vals, rp[k], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_cpp_stiff_tube_matches_oracle(cuda, oracle, tmp_path):
+    """material::StiffFluid<double>{4.4} (p_inf = 0.613, as the reference's
+    one-argument constructor leaves it) through SimulatorImpl."""
+    exe = compile_program(tmp_path, "stiff_tube")
+    out = subprocess.run([exe, str(tmp_path / "stiff")], check=True, capture_output=True,
+                         text=True).stdout
+    iters = int(out.split()[1])
+    data = np.loadtxt(str(tmp_path / "stiff.dat"))
+    n = 200
+    with oracle.stiffened(0.613):
+        u = oracle.fill_riemann((n,), np.array([[1.0, 10.0, 0.0], [1.0, 1.0, 0.0]]), 4.4)
+        ref, steps, rt, _ = oracle.simulate((n,), u, 4.4, 0.9, 0.005, 0.05, 10 ** 9)
+    assert iters == steps
+    rp = oracle.cons_to_prim(ref, 4.4)     # pressure read back as p + gamma p_inf
+    got = data[:, 1:].T
+    assert np.max(np.abs(got - rp) / np.maximum(np.abs(rp), 1e-3)) < 1e-9
