@@ -319,31 +319,29 @@ def run_ours(a, world, rank, local):
     value = world * cells * T * a.steps / (elapsed_ms / 1e3)
 
     # ---- end to end through the C ABI with host buffers ----------------------
+    # fl_host_pipe_run: each step is one whole simulation from a pinned host
+    # state to a pinned host result; job k + 1's upload and job k - 1's
+    # download overlap job k's compute.  Every step's copies are inside the
+    # timed region; the first upload and the last download are not hidden.
+    from fluidity_b200.solver import HostPipeline
     pinned_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
-    pinned_out = torch.empty_like(pinned_in)
     s.fill_riemann(states, out=buf_a)
     pinned_in.copy_(buf_a)
     torch.cuda.synchronize()
     e2e_steps = max(2, min(a.steps, 5))
-
-    def e2e_run():
-        buf_a.copy_(pinned_in, non_blocking=True)
-        res, it2, _ = sim.run(buf_a, buf_b, 0.8, 1.0 / a.size, 1e30, T)
-        pinned_out.copy_(res, non_blocking=True)
-        torch.cuda.synchronize()
-        return it2
-
-    e2e_run()
+    pinned_out = [torch.empty_like(pinned_in) for _ in range(e2e_steps)]
+    pipe = HostPipeline(s, sets=3)
+    pipe.run([pinned_in], pinned_out[:1], 0.8, 1.0 / a.size, 1e30, T)     # warm-up
     barrier(world)
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        it2 = e2e_run()
+    jobs = pipe.run([pinned_in] * e2e_steps, pinned_out, 0.8, 1.0 / a.size, 1e30, T)
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, world, dev)
-    if it2 != T:
+    if any(it2 != T for it2, _ in jobs):
         raise RuntimeError("end-to-end run did not complete")
     e2e_value = world * cells * T * e2e_steps / e2e_s
     state_bytes = nc * elem * cells
+    del pipe
 
     variants = {}
     if not a.no_variants and rank == 0:
@@ -368,7 +366,9 @@ def run_ours(a, world, rank, local):
                      "algorithmic_bytes_per_launch": bytes_per_sweep,
                      "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
-                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "steps": e2e_steps, "api": "fl_host_pipe_run (pinned host in/out)",
+                "overlap": "upload of step k+1 and download of step k-1 run during step k"},
         "gpu_launches": a.steps * (3 + launches_per_run),
         "clocks": clocks,
     }

@@ -94,6 +94,13 @@ PROTOTYPES = {
     "fl_max_wavespeed_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
     "fl_fill_riemann_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
     "fl_sim_set_material": (C.c_int, [_P, C.POINTER(Material)]),
+    "fl_host_pipe_create": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,
+                                      C.c_int]),
+    "fl_host_pipe_destroy": (C.c_int, [_P]),
+    "fl_host_pipe_set_material": (C.c_int, [_P, C.POINTER(Material)]),
+    "fl_host_pipe_run": (C.c_int, [_P, C.c_int32, C.POINTER(_P), C.POINTER(_P), C.c_double,
+                                   C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_double)]),
     "fl_mm_set_materials": (C.c_int, [_P, C.POINTER(Material)]),
     "fl_mm_set_states_mat": (C.c_int, [_G, C.c_uint32, _P, _P, C.POINTER(C.c_double),
                                        C.POINTER(Material), _P]),

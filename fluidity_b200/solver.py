@@ -185,6 +185,53 @@ class Simulation:
         return self._bufs[out.value], int(it.value), float(rt.value)
 
 
+class HostPipeline:
+    """Whole simulations from host memory to host memory (fl_host_pipe_*):
+    job k + 1's upload and job k - 1's download overlap job k's compute.
+    Host tensors should be pinned (``torch.empty(..., pin_memory=True)``) and
+    shaped like ``solver.new_state()``."""
+
+    def __init__(self, solver: SplitSolver, sets: int = 3):
+        self.solver = solver
+        self.lib = solver.lib
+        h = C.c_void_p()
+        capi.check(self.lib.fl_host_pipe_create(C.byref(h), C.byref(solver.grid), solver.gamma,
+                                                solver.policy, solver.boundary_mask, int(sets)),
+                   self.lib)
+        self.handle = h
+        if solver.p_inf != 0.0:
+            capi.check(self.lib.fl_host_pipe_set_material(h, C.byref(solver.material)),
+                       self.lib)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.fl_host_pipe_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def run(self, host_in, host_out, cfl, res, sim_time, max_iters):
+        """host_in / host_out: equal-length lists of pinned host tensors.
+        Returns [(iters, run_time)] per job."""
+        n = len(host_in)
+        if len(host_out) != n:
+            raise ValueError("host_in and host_out differ in length")
+        ins = (C.c_void_p * n)(*[t.data_ptr() for t in host_in])
+        outs = (C.c_void_p * n)(*[t.data_ptr() for t in host_out])
+        for t in list(host_in) + list(host_out):
+            if t.is_cuda or t.numel() * t.element_size() < self.lib.fl_state_bytes(
+                    C.byref(self.solver.grid), self.solver.policy):
+                raise ValueError("host buffers must be host tensors of a whole state")
+        its = (C.c_int64 * max(n, 1))()
+        rts = (C.c_double * max(n, 1))()
+        capi.check(self.lib.fl_host_pipe_run(self.handle, n, ins, outs, float(cfl), float(res),
+                                             float(sim_time), int(max_iters), its, rts),
+                   self.lib)
+        return [(int(its[k]), float(rts[k])) for k in range(n)]
+
+
 def write_separate_raw(u, shape, gamma, prefix, sim_time):
     """write_results_separate_raw (simulator/simulator_impl.hpp:360-420) for a
     host state u ((dims + 2, >= cells) conservative planes): one file per

@@ -187,6 +187,26 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res,
  * launched but do no work. */
 int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream);
 
+/* ---- simulations from host memory to host memory (no reference
+ * counterpart beyond its fill_data / simulate / write_results sequence,
+ * simulator/simulator_impl.hpp:223-358).  fl_host_pipe_run runs njobs
+ * whole simulations of one grid: host_in[k] (a state laid out as on the
+ * device: (dims + 2) planes of `pitch` values) is uploaded, simulated as
+ * fl_simulate would, and its result downloaded to host_out[k].  The upload
+ * of job k + 1 and the download of job k - 1 overlap job k's compute (three
+ * streams; `sets` = 2..4 pairs of device buffers rotate, 3 keeps every
+ * overlap free of shared buffers).  Host buffers should be page-locked.
+ * iters / run_times (nullable) get each job's step count and time.  Returns
+ * after the last download has finished. */
+typedef struct fl_host_pipe fl_host_pipe;
+int fl_host_pipe_create(fl_host_pipe** pipe, const fl_grid* grid, double gamma,
+                        uint32_t policy, uint32_t boundary_mask, int sets);
+int fl_host_pipe_destroy(fl_host_pipe* pipe);
+int fl_host_pipe_set_material(fl_host_pipe* pipe, const fl_material* mat);
+int fl_host_pipe_run(fl_host_pipe* pipe, int32_t njobs, const void* const* host_in,
+                     void* const* host_out, double cfl, double res, double sim_time,
+                     int64_t max_iters, int64_t* iters, double* run_times);
+
 /* ---- one slab of a grid decomposed across GPUs (no reference counterpart:
  * the reference runs one GPU).  A rank holds its own rows (along the slowest
  * dimension) plus ghost rows that the host refreshes from the neighbouring

@@ -158,6 +158,10 @@ def _stiff_err(out, ref, u, gamma, dtdh):
     p_state = np.max(np.abs((gamma - 1.0) * (u[1] - 0.5 * u[0] * v2)))
     a = np.asarray(out, dtype=np.float64)
     b = np.asarray(ref, dtype=np.float64)
+    na, nb = np.isnan(a), np.isnan(b)
+    if (na != nb).any():
+        return float("inf")                 # NaN in one result only
+    a, b = np.where(na, 0.0, a), np.where(nb, 0.0, b)
     scale = np.max(np.abs(b), axis=1, keepdims=True)
     den = np.maximum(np.abs(b), 1e-3 * scale) + dtdh * p_state
     return float(np.max(np.abs(a - b) / den))
