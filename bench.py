@@ -329,7 +329,8 @@ def run_ours(a, world, rank, local):
     pinned_in.copy_(buf_a)
     torch.cuda.synchronize()
     e2e_steps = max(2, min(a.steps, 5))
-    pinned_out = [torch.empty_like(pinned_in) for _ in range(e2e_steps)]
+    pinned_out = [torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
+                  for _ in range(e2e_steps)]
     pipe = HostPipeline(s, sets=3)
     pipe.run([pinned_in], pinned_out[:1], 0.8, 1.0 / a.size, 1e30, T)     # warm-up
     barrier(world)
@@ -727,7 +728,7 @@ def run_slabs(a, world, rank, local):
 
     # end to end: the slab from pinned host memory, the run, the slab back
     pin_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
-    pin_out = torch.empty_like(pin_in)
+    pin_out = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
     pin_in.copy_(init)
     e2e_steps = max(2, min(a.steps, 5))
 

@@ -90,8 +90,11 @@ __device__ __forceinline__ int64_t mirror_index(int64_t g, int64_t n, bool& flip
   return g;
 }
 
+// acc = max(acc, v), except that a NaN, once seen, stays: a non-finite
+// wavespeed anywhere must reach the step control (which stops the loop with
+// FL_ENAN), whatever the order in which cells and lanes are folded.
 __device__ __forceinline__ void ws_max(double& acc, double v) {
-  if (!(v <= acc)) acc = v;  // NaN propagates
+  if (acc == acc && !(v <= acc)) acc = v;
 }
 
 // Advance the time control after the last sweep of a step

@@ -334,6 +334,24 @@ def test_nan_state_reports_enan(cuda):
     assert e.value.code == capi.FL_ENAN
 
 
+@pytest.mark.parametrize("where", [(100, 77), (0, 0), (255, 255), (31, 130)])
+def test_nan_anywhere_reports_enan(cuda, where):
+    """A NaN in one cell of a 2-D state stops the loop with FL_ENAN whatever
+    position it has in the kernels' fold order (initial wavespeed, fused
+    per-lane, warp and CTA maxima)."""
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.solver import Simulation, SplitSolver
+    s = SplitSolver((256, 256), gamma=GAMMA)
+    a = s.fill_riemann(np.array([[1.0, 1.0, 0.0, 0.0], [0.5, 0.4, 0.1, 0.0],
+                                 [0.8, 0.6, 0.0, 0.1], [0.3, 0.3, 0.0, 0.0]]))
+    a[1, where[1] * 256 + where[0]] = float("nan")
+    b = torch.empty_like(a)
+    with pytest.raises(capi.FlError) as e:
+        Simulation(s).run(a, b, 0.8, 1 / 256, 1e30, 2)
+    assert e.value.code == capi.FL_ENAN
+
+
 def test_split_solve_swaps_like_reference(cuda, oracle):
     import torch
     from fluidity_b200.solver import SplitSolver
