@@ -18,8 +18,9 @@
 //    relaxes to the fixed point of the Godunov local eikonal solve
 //    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles relax in shared
 //    memory, passes ping-pong between two buffers, only tiles stamped by a
-//    changed neighbour relax in the next pass (the others copy), and the
-//    host checks convergence once per 16 passes; the result takes the
+//    changed neighbour relax in the next pass (a worklist; the others hold
+//    the same values in both buffers), and the host checks convergence once
+//    per 16 passes; the result takes the
 //    input's sign (set_signs, :96-112).
 // FP64 level sets on 2-D grids; out-of-domain reads mirror the domain.
 #include <cuda_runtime.h>
@@ -207,54 +208,49 @@ __device__ __forceinline__ double eik_local(double xm, double xp, double ym, dou
   return 0.5 * (a + b + sqrt(2.0 * fh * fh - (amb * amb)));
 }
 
-// Pass k over the tiles: reads src (the previous pass) and writes dst.  A
-// tile relaxes in pass 0 and in every pass whose number its stamp has
-// reached (a changed tile stamps itself and its eight neighbours with k + 1);
-// it loads itself and a one-cell halo (+max outside the domain), relaxes
-// FIM_INNER rounds in shared memory and writes its cells to dst.  A tile that
-// does not relax must hand its values on to dst; it copies them unless both
-// buffers already hold them (synced[t]: set when a tile copies or relaxes
-// without change, cleared when it changes).  Every pass depends only on the
-// previous one, so the result is deterministic.  CTAs loop over the tiles.
-// A pass after one that changed nothing returns at once (last_change < k - 1)
-// without writing.
+// Pass k over a worklist of tiles: reads src (the previous pass) and writes
+// dst.  Pass 0 relaxes every tile; pass k > 0 relaxes the tiles that a tile
+// which changed in pass k - 1 stamped (itself and its eight neighbours),
+// each listed once.  A relaxing tile loads itself and a one-cell halo (+max
+// outside the domain), relaxes FIM_INNER rounds in shared memory and writes
+// its cells to dst.  A tile off the list holds the same values in both
+// buffers: it last relaxed without a change (a tile that changes always
+// relaxes again in the next pass), so it needs no copy.  Every pass depends
+// only on the previous one, so the result is deterministic.
+//   lists:  3 lists of up to `tiles` entries; pass k reads list k % 3,
+//           appends to list (k + 1) % 3 and clears the count of list
+//           (k + 2) % 3, which pass k - 1 has finished with.
+//   counts: the 3 list lengths.
+// A pass after one that changed nothing returns at once (last_change < k - 1).
 __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     const double* __restrict__ src, double* __restrict__ dst,
     const unsigned char* __restrict__ fixed, int64_t nx, int64_t ny, double h,
-    int* __restrict__ stamp, int* __restrict__ synced, int tiles_x, int tiles_y,
-    int* __restrict__ last_change, int k) {
+    int* __restrict__ stamp, int* __restrict__ lists, int* __restrict__ counts, int tiles_x,
+    int tiles_y, int* __restrict__ last_change, int k) {
   if (k > 0 && *(volatile int*)last_change < k - 1) return;
   __shared__ double s[FT + 2][FT + 2];
   __shared__ int changed;
-  __shared__ int mode;   // 0: relax, 1: copy, 2: nothing to do
   const int lx = threadIdx.x % FT, ly = threadIdx.x / FT;
   const int tiles = tiles_x * tiles_y;
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+  const int* list = lists + (k % 3) * tiles;
+  int* next = lists + ((k + 1) % 3) * tiles;
+  int* next_count = counts + (k + 1) % 3;
+  if (blockIdx.x == 0 && threadIdx.x == 0) counts[(k + 2) % 3] = 0;
+  const int count = (k == 0) ? tiles : *(volatile int*)(counts + k % 3);
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const int t = (k == 0) ? i : list[i];
     const int tx0 = t % tiles_x, ty0 = t / tiles_x;
     const int64_t x = (int64_t)tx0 * FT + lx, y = (int64_t)ty0 * FT + ly;
     const bool in = x < nx && y < ny;
-    const int64_t i = y * nx + x;
-    // a neighbour may raise stamp[t] during this pass: one thread reads it
-    // and the whole CTA follows that reading
-    if (threadIdx.x == 0) {
-      const int st = *(volatile int*)(stamp + t);
-      mode = (k == 0 || st >= k) ? 0 : (synced[t] ? 2 : 1);
-      changed = 0;
-    }
-    __syncthreads();
-    if (mode != 0) {
-      if (mode == 1 && in) dst[i] = src[i];
-      if (mode == 1 && threadIdx.x == 0) synced[t] = 1;
-      __syncthreads();   // mode is rewritten for the next tile
-      continue;
-    }
+    const int64_t ci = y * nx + x;
+    if (threadIdx.x == 0) changed = 0;
     for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
       const int hx = q % (FT + 2), hy = q / (FT + 2);
       const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
       s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
     }
     __syncthreads();
-    const bool free_cell = in && !fixed[i];
+    const bool free_cell = in && !fixed[ci];
     bool mine = false;
     for (int r = 0; r < FIM_INNER; ++r) {
       double q = 0.0;
@@ -267,20 +263,18 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
       }
       __syncthreads();
     }
-    if (in) dst[i] = s[ly + 1][lx + 1];
+    if (in) dst[ci] = s[ly + 1][lx + 1];
     if (mine) changed = 1;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      synced[t] = changed ? 0 : 1;
-      if (changed) {
-        atomicMax(last_change, k);
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -1; dx <= 1; ++dx) {
-            const int ax = tx0 + dx, ay = ty0 + dy;
-            if (ax >= 0 && ax < tiles_x && ay >= 0 && ay < tiles_y)
-              stamp[ay * tiles_x + ax] = k + 1;
-          }
-      }
+    if (threadIdx.x == 0 && changed) {
+      atomicMax(last_change, k);
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int ax = tx0 + dx, ay = ty0 + dy;
+          if (ax < 0 || ax >= tiles_x || ay < 0 || ay >= tiles_y) continue;
+          const int nt = ay * tiles_x + ax;
+          if (atomicMax(stamp + nt, k + 1) < k + 1) next[atomicAdd(next_count, 1)] = nt;
+        }
     }
     __syncthreads();   // s and changed are reused by the next tile
   }
@@ -321,10 +315,11 @@ int64_t fl_ls_workspace_bytes(const fl_grid* grid) {
   const int64_t n = grid->n[0] * grid->n[1];
   const int64_t tiles = ((grid->n[0] + FT - 1) / FT) * ((grid->n[1] + FT - 1) / FT);
   // two FP64 planes (RK3 stages; the first also the reinitialisation's
-  // second buffer), its fixed-cell flags, tile stamps (room for two ints per
-  // tile) and change counter, each 256-byte aligned
+  // second buffer), its fixed-cell flags, tile stamps, three tile
+  // worklists, and the change counter with the list counts, each 256-byte
+  // aligned
   auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
-  return al(2 * n * 8) + al(n) + al(2 * tiles * 4) + 256;
+  return al(2 * n * 8) + al(n) + al(tiles * 4) + al(3 * tiles * 4) + 256;
 }
 
 int fl_ls_velocity(const fl_grid* grid, int nmat, const double* const* phis,
@@ -398,13 +393,16 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
   char* w = static_cast<char*>(workspace);
   unsigned char* fixed = reinterpret_cast<unsigned char*>(w + al(2 * n * 8));
   int* stamp = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n));
-  int* last = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(2 * tiles * 4));
+  int* lists = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(tiles * 4));
+  int* last = reinterpret_cast<int*>(w + al(2 * n * 8) + al(n) + al(tiles * 4) +
+                                     al(3 * tiles * 4));
+  int* counts = last + 1;
   // passes ping-pong between `out` (even passes read it) and the first
   // workspace plane
   double* buf[2] = {out, reinterpret_cast<double*>(w)};
   fim_init_kernel<<<grid1d(n), 256, 0, st>>>(phi, nx, ny, out, fixed);
-  fill_int_kernel<<<grid1d(2 * tiles), 256, 0, st>>>(stamp, 2 * tiles, 0);  // stamps, synced
-  fill_int_kernel<<<1, 32, 0, st>>>(last, 1, 0);
+  fill_int_kernel<<<grid1d(tiles), 256, 0, st>>>(stamp, tiles, 0);
+  fill_int_kernel<<<1, 32, 0, st>>>(last, 4, 0);   // last change, 3 list counts
   // passes are launched in chunks; the host reads the last pass that changed
   // anything after each chunk (passes past convergence return at once)
   constexpr int CHUNK = 16;
@@ -420,7 +418,7 @@ int fl_ls_reinit(const fl_grid* grid, const double* phi, double h, double* out, 
     const int end = launched + CHUNK < max_passes ? launched + CHUNK : max_passes;
     for (int k = launched; k < end; ++k)
       fim_pass_kernel<<<pass_ctas, FT * FT, 0, st>>>(buf[k & 1], buf[(k + 1) & 1], fixed, nx, ny,
-                                                     h, stamp, stamp + tiles, tiles_x, tiles_y,
+                                                     h, stamp, lists, counts, tiles_x, tiles_y,
                                                      last, k);
     launched = end;
     e = cudaGetLastError();
