@@ -252,16 +252,19 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     __syncthreads();
     const bool free_cell = in && !fixed[ci];
     bool mine = false;
+    // up to FIM_INNER rounds; a round that changes no cell of the tile ends
+    // them (the next round would see the same values: same result)
     for (int r = 0; r < FIM_INNER; ++r) {
       double q = 0.0;
       if (free_cell)
         q = eik_local(s[ly + 1][lx], s[ly + 1][lx + 2], s[ly][lx + 1], s[ly + 2][lx + 1], h);
       __syncthreads();
-      if (free_cell && q < s[ly + 1][lx + 1]) {
+      const bool upd = free_cell && q < s[ly + 1][lx + 1];
+      if (upd) {
         s[ly + 1][lx + 1] = q;
         mine = true;
       }
-      __syncthreads();
+      if (!__syncthreads_or(upd)) break;
     }
     if (in) dst[ci] = s[ly + 1][lx + 1];
     if (mine) changed = 1;
