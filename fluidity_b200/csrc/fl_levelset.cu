@@ -74,8 +74,11 @@ constexpr int SX = LX + 2 * LH, SY = LY + 2 * LH;
 //   stage 1: out = phi_n - dt H(phi_n)
 //   stage 2: out = 0.75 phi_n + 0.25 (s - dt H(s))
 //   stage 3: out = (1/3) phi_n + (2/3) (s - dt H(s))
+#ifndef FL_LS_RK3_CTAS
+#define FL_LS_RK3_CTAS 1
+#endif
 template <int STAGE>
-__global__ void __launch_bounds__(LX * LY) ls_rk3_kernel(const double* __restrict__ phi_n,
+__global__ void __launch_bounds__(LX * LY, FL_LS_RK3_CTAS) ls_rk3_kernel(const double* __restrict__ phi_n,
                                                          const double* __restrict__ s,
                                                          const double* __restrict__ vel,
                                                          double dt, double h, int64_t nx,

@@ -36,7 +36,13 @@ struct MMCounters {
   int band[2];     // band cells per material
   int gfm[2];      // GFM targets per material
   int iters[2];    // Jacobi sweeps of the last extrapolation
-  int pad[2];
+  int stop[2];     // 1 once the material's extrapolation has converged
+  // the extrapolation sweep in flight: max change (bits of a non-negative
+  // double) and NaN flag per material and sweep parity, blocks arrived
+  unsigned long long err[2][2];
+  int nan[2][2];
+  unsigned int arrive;
+  int pad;
 };
 
 struct MMArgs {
@@ -211,17 +217,27 @@ __global__ void __launch_bounds__(256) mm_scan_kernel(MMArgs a) {
         const int slot = atomicAdd(&a.cnt->band[m], 1);
         a.band_list[m][slot] = (int)t;
       }
-      // pull: the last source in raster order whose target is this cell
+      // pull: the last source in raster order whose target is this cell.
+      // The 8 neighbours' level-set values are loaded together first; a cell
+      // with no neighbour in [-h, 0] (almost every cell) is done after one
+      // round trip.
+      unsigned cand = 0u;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        const int dx = 1 - q % 3, dy = 1 - q / 3;
+        const int64_t cx = x + dx, cy = y + dy;
+        if (q == 4 || cx < 0 || cx >= a.nx || cy < 0 || cy >= a.ny) continue;
+        const double ps = pa[cy * a.nx + cx];
+        if (ps <= 0.0 && ps >= -a.h) cand |= 1u << q;
+      }
       bool found = false;
       double nrm[2] = {0.0, 0.0};
       int64_t sx = 0, sy = 0;
-      for (int dy = 1; dy >= -1 && !found; --dy) {
+      for (int dy = 1; dy >= -1 && !found && cand; --dy) {
         for (int dx = 1; dx >= -1 && !found; --dx) {
           if (dx == 0 && dy == 0) continue;
           const int64_t cx = x + dx, cy = y + dy;
-          if (cx < 0 || cx >= a.nx || cy < 0 || cy >= a.ny) continue;
-          const double ps = pa[cy * a.nx + cx];
-          if (!(ps <= 0.0 && ps >= -a.h)) continue;
+          if (!(cand & (1u << ((1 - dy) * 3 + (1 - dx))))) continue;
           double nn[2];
           if (!gfm_source(pa, pb, a.nx, a.ny, cx, cy, a.h, nn)) continue;
           if (cx + isgn(nn[0]) != x || cy + isgn(nn[1]) != y) continue;
@@ -258,104 +274,123 @@ __global__ void mm_scatter_kernel(MMArgs a) {
   }
 }
 
-constexpr int EX_THREADS = 1024;
-
-// One CTA per material (blockIdx.x): Jacobi sweeps of the ghost-cell
-// extrapolation (ghost_fluid_extrapolator.hpp:99-196) over the band list.
+// Ghost-cell extrapolation (ghost_fluid_extrapolator.hpp:99-196) as Jacobi
+// sweeps over the band lists of both materials, one launch per sweep, one
+// thread per band cell.  Sweep `it` (counted from `base`, the sweeps done
+// before this chunk) reads the iterate from U (even) or X (odd) and writes
+// the other buffer; neighbours outside the band read U.  The last block to
+// finish a sweep closes it: a material whose largest change is below 1e-8
+// with no NaN stops (later sweeps skip it), and its sweep count is recorded.
+// mm_extrap_finish_kernel then moves a final iterate left in X back to U.
 template <typename T>
-__global__ void __launch_bounds__(EX_THREADS) mm_extrap_kernel(MMArgs a) {
-  const int m = blockIdx.x;
-  const int cnt = a.cnt->band[m];
-  const int* list = a.band_list[m];
-  const double* phi = a.phi[m];
-  T* U = static_cast<T*>(a.w[m]);
-  T* X = static_cast<T*>(a.x[m]);
+__global__ void __launch_bounds__(256) mm_extrap_sweep_kernel(MMArgs a, int it, int base) {
+  MMCounters* c = a.cnt;
+  const int n0 = c->band[0], n1 = c->band[1];
+  const int par = (it - base) & 1;
   const int64_t nx = a.nx, ny = a.ny, pitch = a.pitch;
   const double h = a.h;
-  __shared__ double s_err[EX_THREADS / 32];
-  __shared__ int s_stop;
-  int it = 0;
-  bool final_in_x = false;
-  for (; it < a.max_iters;) {
-    const T* src = (it & 1) ? X : U;  // band cells of the current iterate
-    T* dst = (it & 1) ? U : X;
-    double worst = 0.0;
-    int nan_seen = 0;
-    for (int k = threadIdx.x; k < cnt; k += EX_THREADS) {
-      const int64_t i = list[k];
-      const int64_t x = i % nx, y = i / nx;
-      const double fact = 0.5 / h;
-      double g[2];
-      g[0] = fact * (phi[midx(nx, ny, x + 1, y)] - phi[midx(nx, ny, x - 1, y)]);
-      g[1] = fact * (phi[midx(nx, ny, x, y + 1)] - phi[midx(nx, ny, x, y - 1)]);
-      const double s = sqrt(g[0] * g[0] + g[1] * g[1]);
-      const double sign = (double)isgn(phi[i]);
-      double nrm[2], l1 = 0.0;
+  double worst[2] = {0.0, 0.0};
+  int nan_seen[2] = {0, 0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n0 + n1; k += gridDim.x * blockDim.x) {
+    const int m = k < n0 ? 0 : 1;
+    if (*(volatile int*)&c->stop[m]) continue;
+    const int64_t i = a.band_list[m][m == 0 ? k : k - n0];
+    const double* phi = a.phi[m];
+    T* U = static_cast<T*>(a.w[m]);
+    T* X = static_cast<T*>(a.x[m]);
+    const T* src = par ? X : U;
+    T* dst = par ? U : X;
+    const int64_t x = i % nx, y = i / nx;
+    const double fact = 0.5 / h;
+    double g[2];
+    g[0] = fact * (phi[midx(nx, ny, x + 1, y)] - phi[midx(nx, ny, x - 1, y)]);
+    g[1] = fact * (phi[midx(nx, ny, x, y + 1)] - phi[midx(nx, ny, x, y - 1)]);
+    const double sq = sqrt(g[0] * g[0] + g[1] * g[1]);
+    const double sign = (double)isgn(phi[i]);
+    double nrm[2], l1 = 0.0;
 #pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        nrm[d] = -sign * (g[d] / s);
-        l1 += fabs(nrm[d]);
-      }
-      const bool use_n = l1 > 1e-2;
-      double p[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        const int64_t qm = d == 0 ? midx(nx, ny, x - 1, y) : midx(nx, ny, x, y - 1);
-        const int64_t qp = d == 0 ? midx(nx, ny, x + 1, y) : midx(nx, ny, x, y + 1);
-        const int64_t q = phi[qm] < phi[qp] ? qm : qp;
-        const T* from = in_band(phi[q], h) ? src : U;
-        const double wgt = use_n ? fabs(nrm[d]) : 0.5;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) p[c] += (double)from[c * pitch + q] * wgt;
-      }
-      if (use_n) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) p[c] = p[c] / l1;
-      }
-      bool has_nan = false;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) has_nan |= isnan(p[c]);
-      double err = 0.0;
-      if (has_nan) {
-        nan_seen = 1;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) dst[c * pitch + i] = src[c * pitch + i];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const T v = (T)p[c];
-          err += fabs((double)v - (double)src[c * pitch + i]);
-          dst[c * pitch + i] = v;
-        }
-      }
-      worst = (err > worst) ? err : worst;
+    for (int d = 0; d < 2; ++d) {
+      nrm[d] = -sign * (g[d] / sq);
+      l1 += fabs(nrm[d]);
     }
+    const bool use_n = l1 > 1e-2;
+    double pv[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double o = __shfl_xor_sync(0xffffffffu, worst, off);
-      worst = (o > worst) ? o : worst;
+    for (int d = 0; d < 2; ++d) {
+      const int64_t qm = d == 0 ? midx(nx, ny, x - 1, y) : midx(nx, ny, x, y - 1);
+      const int64_t qp = d == 0 ? midx(nx, ny, x + 1, y) : midx(nx, ny, x, y + 1);
+      const int64_t q = phi[qm] < phi[qp] ? qm : qp;
+      const T* from = in_band(phi[q], h) ? src : U;
+      const double wgt = use_n ? fabs(nrm[d]) : 0.5;
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) pv[cc] += (double)from[cc * pitch + q] * wgt;
     }
-    const int any_nan = __syncthreads_or(nan_seen);
-    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = worst;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mx = 0.0;
-      for (int w = 0; w < EX_THREADS / 32; ++w) mx = (s_err[w] > mx) ? s_err[w] : mx;
-      s_stop = (!(mx >= 1e-8) && !any_nan) ? 1 : 0;
+    if (use_n) {
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) pv[cc] = pv[cc] / l1;
     }
-    __syncthreads();
-    ++it;
-    final_in_x = (it & 1) != 0;
-    if (s_stop) break;
+    bool has_nan = false;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) has_nan |= isnan(pv[cc]);
+    double err = 0.0;
+    if (has_nan) {
+      nan_seen[m] = 1;
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) dst[cc * pitch + i] = src[cc * pitch + i];
+    } else {
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const T v = (T)pv[cc];
+        err += fabs((double)v - (double)src[cc * pitch + i]);
+        dst[cc * pitch + i] = v;
+      }
+    }
+    worst[m] = (err > worst[m]) ? err : worst[m];
   }
-  if (final_in_x) {
-    for (int k = threadIdx.x; k < cnt; k += EX_THREADS) {
-      const int64_t i = list[k];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) U[c * pitch + i] = X[c * pitch + i];
+  for (int m = 0; m < 2; ++m) {
+    if (worst[m] > 0.0)
+      atomicMax(&c->err[m][par], (unsigned long long)__double_as_longlong(worst[m]));
+    if (nan_seen[m]) atomicOr(&c->nan[m][par], 1);
+  }
+  __threadfence();   // this thread's writes and atomics, before the block arrives
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(&c->arrive, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        volatile MMCounters* vc = c;
+        if (vc->stop[m]) continue;
+        const double mx = __longlong_as_double((long long)vc->err[m][par]);
+        vc->iters[m] = it + 1;
+        if (!(mx >= 1e-8) && !vc->nan[m][par]) vc->stop[m] = 1;
+        vc->err[m][1 - par] = 0ull;
+        vc->nan[m][1 - par] = 0;
+      }
+      c->arrive = 0u;
     }
   }
-  if (threadIdx.x == 0) a.cnt->iters[m] = it;
+}
+
+// After a chunk of sweeps: a material whose last iterate is in X (an odd
+// number of sweeps in the chunk since U held the iterate) gets its band
+// cells copied back to U.
+template <typename T>
+__global__ void __launch_bounds__(256) mm_extrap_finish_kernel(MMArgs a, int base) {
+  MMCounters* c = a.cnt;
+  const int n0 = c->band[0], n1 = c->band[1];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n0 + n1; k += gridDim.x * blockDim.x) {
+    const int m = k < n0 ? 0 : 1;
+    if (((c->iters[m] - base) & 1) == 0 || c->iters[m] <= base) continue;
+    const int64_t i = a.band_list[m][m == 0 ? k : k - n0];
+    T* U = static_cast<T*>(a.w[m]);
+    const T* X = static_cast<const T*>(a.x[m]);
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) U[cc * a.pitch + i] = X[cc * a.pitch + i];
+  }
 }
 
 template <typename T>
@@ -427,6 +462,9 @@ struct fl_mm {
   int done, status;
   int extrap_iters;
   int stats[8];
+  MMArgs ghost_args;   // the last ghost pass, for its extrapolation's continuation
+  int ex_launched;     // extrapolation sweeps launched in the last ghost pass
+  int ex_max;          // its sweep limit
 };
 
 namespace {
@@ -449,7 +487,46 @@ int cuda_err(cudaError_t e, const char* where) {
   return set_error(kECuda, "%s: %s", where, cudaGetErrorString(e));
 }
 
-// GFM + extrapolation on states u[m] with second buffers x[m].
+constexpr int kExChunk = 8;   // extrapolation sweeps launched before the host looks
+
+// One chunk of extrapolation sweeps, starting at sweep m->ex_launched with the
+// iterate in U, then the copy-back of iterates left in X.
+cudaError_t extrap_chunk(fl_mm* m, cudaStream_t st) {
+  const MMArgs& a = m->ghost_args;
+  const int base = m->ex_launched;
+  const int end = base + kExChunk < m->ex_max ? base + kExChunk : m->ex_max;
+  const unsigned blocks = 148 * 2;
+  for (int it = base; it < end; ++it) {
+    if (m->f32) mm_extrap_sweep_kernel<float><<<blocks, 256, 0, st>>>(a, it, base);
+    else mm_extrap_sweep_kernel<double><<<blocks, 256, 0, st>>>(a, it, base);
+  }
+  if (m->f32) mm_extrap_finish_kernel<float><<<blocks, 256, 0, st>>>(a, base);
+  else mm_extrap_finish_kernel<double><<<blocks, 256, 0, st>>>(a, base);
+  m->ex_launched = end;
+  return cudaGetLastError();
+}
+
+// Whether the last ghost pass's extrapolation still has sweeps to run
+// (reads the counters; the caller has synchronised the stream).
+bool extrap_unfinished(const fl_mm* m, const MMCounters& c) {
+  return m->ex_launched < m->ex_max && (!c.stop[0] || !c.stop[1]);
+}
+
+// Runs the remaining chunks of the last ghost pass's extrapolation, waiting
+// for the stream after each.
+int extrap_complete(fl_mm* m, cudaStream_t st) {
+  for (;;) {
+    MMCounters c;
+    cudaError_t e = cudaMemcpyAsync(&c, m->cnt, sizeof(c), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(e, "fl_mm extrapolation");
+    if (!extrap_unfinished(m, c)) return kOk;
+    if ((e = extrap_chunk(m, st)) != cudaSuccess) return cuda_err(e, "fl_mm extrapolation");
+  }
+}
+
+// GFM + the first chunk of the extrapolation on states u[m] with second
+// buffers x[m].
 int ghost_pass(fl_mm* m, void* const* u, void* const* x, const double* const* phi, int max_iters,
                cudaStream_t st) {
   MMArgs a;
@@ -477,13 +554,15 @@ int ghost_pass(fl_mm* m, void* const* u, void* const* x, const double* const* ph
   if (m->f32) {
     mm_scan_kernel<float><<<grid_for(n), 256, 0, st>>>(a);
     mm_scatter_kernel<float><<<148, 256, 0, st>>>(a);
-    mm_extrap_kernel<float><<<2, EX_THREADS, 0, st>>>(a);
   } else {
     mm_scan_kernel<double><<<grid_for(n), 256, 0, st>>>(a);
     mm_scatter_kernel<double><<<148, 256, 0, st>>>(a);
-    mm_extrap_kernel<double><<<2, EX_THREADS, 0, st>>>(a);
   }
+  m->ghost_args = a;
+  m->ex_launched = 0;
+  m->ex_max = max_iters;
   e = cudaGetLastError();
+  if (e == cudaSuccess) e = extrap_chunk(m, st);
   if (e != cudaSuccess) return cuda_err(e, "fl_mm ghost");
   return kOk;
 }
@@ -544,7 +623,9 @@ int fl_mm_ghost(fl_mm* m, void* u0, void* u1, void* scratch0, void* scratch1, co
   void* u[2] = {u0, u1};
   void* x[2] = {scratch0, scratch1};
   const double* p[2] = {phi0, phi1};
-  return ghost_pass(m, u, x, p, max_iters, static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int rc = ghost_pass(m, u, x, p, max_iters, st);
+  return rc ? rc : extrap_complete(m, st);
 }
 
 int fl_mm_stats(const fl_mm* m, int32_t* out, int32_t n) {
@@ -682,16 +763,26 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     const double* p[2] = {m->phi[0][m->phi_cur[0]], m->phi[1][m->phi_cur[1]]};
     int rc = ghost_pass(m, u, x, p, m->extrap_iters, st);
     if (rc) return rc;
-    // 3: time step over both materials (multimaterial_simulator.hpp:384-404)
-    for (int mat = 0; mat < 2; ++mat) {
-      const fl_material mm{m->gamma[mat], m->pinf[mat]};
-      rc = fl_max_wavespeed_mat(g, u[mat], &mm, m->policy, m->ws_dev + mat, stream);
-      if (rc) return rc;
-    }
+    // 3: time step over both materials (multimaterial_simulator.hpp:384-404).
+    // The host reads the wavespeeds and, with them, whether the ghost pass's
+    // extrapolation converged within its first chunk of sweeps; if not, the
+    // remaining sweeps run and the wavespeeds are taken again.
     double ws[2];
-    cudaError_t e = cudaMemcpyAsync(ws, m->ws_dev, sizeof(ws), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_err(e, "fl_mm_steps");
+    cudaError_t e = cudaSuccess;
+    for (;;) {
+      for (int mat = 0; mat < 2; ++mat) {
+        const fl_material mm{m->gamma[mat], m->pinf[mat]};
+        rc = fl_max_wavespeed_mat(g, u[mat], &mm, m->policy, m->ws_dev + mat, stream);
+        if (rc) return rc;
+      }
+      MMCounters cnt;
+      e = cudaMemcpyAsync(ws, m->ws_dev, sizeof(ws), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, m->cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return cuda_err(e, "fl_mm_steps");
+      if (!extrap_unfinished(m, cnt)) break;
+      if ((rc = extrap_complete(m, st))) return rc;
+    }
     const double w = (ws[0] < ws[1]) ? ws[1] : ws[0];
     if (!(w > 0.0) || !(w <= DBL_MAX)) {
       m->done = 1;
