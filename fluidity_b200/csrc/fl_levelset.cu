@@ -75,7 +75,7 @@ constexpr int SX = LX + 2 * LH, SY = LY + 2 * LH;
 //   stage 2: out = 0.75 phi_n + 0.25 (s - dt H(s))
 //   stage 3: out = (1/3) phi_n + (2/3) (s - dt H(s))
 #ifndef FL_LS_RK3_CTAS
-#define FL_LS_RK3_CTAS 1
+#define FL_LS_RK3_CTAS 4   // 64 registers: 4 CTAs per SM (measured 8% faster than 3 at 74)
 #endif
 template <int STAGE>
 __global__ void __launch_bounds__(LX * LY, FL_LS_RK3_CTAS) ls_rk3_kernel(const double* __restrict__ phi_n,

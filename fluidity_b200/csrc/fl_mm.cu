@@ -203,12 +203,14 @@ __device__ __forceinline__ bool in_band(double phi, double h) {
   return phi > 0.0 && phi <= upper && phi >= h;
 }
 
+// One thread per cell: x from blockIdx.x, rows from blockIdx.y (strided when
+// the grid has more rows than a launch's y extent).
 template <typename T>
 __global__ void __launch_bounds__(256) mm_scan_kernel(MMArgs a) {
-  const int64_t n = a.nx * a.ny;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t x = t % a.nx, y = t / a.nx;
+  const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.nx) return;
+  for (int64_t y = blockIdx.y; y < a.ny; y += gridDim.y) {
+    const int64_t t = y * a.nx + x;
 #pragma unroll 1
     for (int m = 0; m < 2; ++m) {
       const double* pa = a.phi[m];
@@ -393,6 +395,12 @@ __global__ void __launch_bounds__(256) mm_extrap_finish_kernel(MMArgs a, int bas
   }
 }
 
+__global__ void negate_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = -src[i];
+}
+
 template <typename T>
 __global__ void set_states_kernel(T* u, int64_t pitch, int64_t n, const double* phi, T c0, T c1,
                                   T c2, T c3) {
@@ -548,14 +556,14 @@ int ghost_pass(fl_mm* m, void* const* u, void* const* x, const double* const* ph
   }
   a.cnt = m->cnt;
   a.max_iters = max_iters;
-  const int64_t n = a.nx * a.ny;
   cudaError_t e = cudaMemsetAsync(m->cnt, 0, sizeof(MMCounters), st);
   if (e != cudaSuccess) return cuda_err(e, "fl_mm ghost");
+  const dim3 scan_grid((unsigned)((a.nx + 255) / 256), (unsigned)(a.ny < 65535 ? a.ny : 65535));
   if (m->f32) {
-    mm_scan_kernel<float><<<grid_for(n), 256, 0, st>>>(a);
+    mm_scan_kernel<float><<<scan_grid, 256, 0, st>>>(a);
     mm_scatter_kernel<float><<<148, 256, 0, st>>>(a);
   } else {
-    mm_scan_kernel<double><<<grid_for(n), 256, 0, st>>>(a);
+    mm_scan_kernel<double><<<scan_grid, 256, 0, st>>>(a);
     mm_scatter_kernel<double><<<148, 256, 0, st>>>(a);
   }
   m->ghost_args = a;
@@ -814,15 +822,22 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     if (rc) return rc;
     const bool reinit = m->reinit_every > 0 && ((m->iters + 1) % m->reinit_every) == 0;
     if (reinit) {
-      for (int mat = 0; mat < 2; ++mat) {
-        const int c = m->phi_cur[mat];
-        int passes = 0;
-        rc = fl_ls_reinit(g, m->phi[mat][c], m->h, m->phi[mat][1 - c], m->ls_ws, 1 << 20, &passes,
-                          stream);
-        if (rc) return rc;
-        m->stats[6 + mat] = passes;
-        m->phi_cur[mat] = 1 - c;
-      }
+      // The projection has just set phi1 = -phi0 exactly, and the
+      // reinitialisation is odd bit for bit (sources keep |phi|, the passes
+      // see only distances, the sign is applied last): reinit(phi1) is the
+      // negation of reinit(phi0), so material 1 takes that instead of a
+      // second run.
+      const int c0 = m->phi_cur[0], c1 = m->phi_cur[1];
+      int passes = 0;
+      rc = fl_ls_reinit(g, m->phi[0][c0], m->h, m->phi[0][1 - c0], m->ls_ws, 1 << 20, &passes,
+                        stream);
+      if (rc) return rc;
+      negate_kernel<<<grid_for(n), 256, 0, st>>>(n, m->phi[0][1 - c0], m->phi[1][1 - c1]);
+      cudaError_t ne = cudaGetLastError();
+      if (ne != cudaSuccess) return cuda_err(ne, "fl_mm_steps");
+      m->stats[6] = m->stats[7] = passes;
+      m->phi_cur[0] = 1 - c0;
+      m->phi_cur[1] = 1 - c1;
     }
     // 6: time bookkeeping (sim/parameters.hpp:60-77)
     m->run_time += dt;
