@@ -247,13 +247,14 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
     const bool in = x < nx && y < ny;
     const int64_t ci = y * nx + x;
     if (threadIdx.x == 0) changed = 0;
+    // the cell's fixed flag is loaded with the tile, before the barrier
+    const bool free_cell = in && !fixed[ci];
     for (int q = threadIdx.x; q < (FT + 2) * (FT + 2); q += FT * FT) {
       const int hx = q % (FT + 2), hy = q / (FT + 2);
       const int64_t gx = (int64_t)tx0 * FT + hx - 1, gy = (int64_t)ty0 * FT + hy - 1;
       s[hy][hx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? src[gy * nx + gx] : DBL_MAX;
     }
     __syncthreads();
-    const bool free_cell = in && !fixed[ci];
     bool mine = false;
     // up to FIM_INNER rounds; a round that changes no cell of the tile ends
     // them (the next round would see the same values: same result)
