@@ -59,11 +59,22 @@ struct AdjGeom {
   static constexpr int E = E0 * E1;
   static constexpr int OUT = T0 * T1;
   static constexpr int THREADS = TS_::THREADS;
+  // CTAs per SM the registers are held to (shared memory allows 2 in FP64,
+  // 4 or 5 in FP32)
+#ifndef FL_ADJ_CTAS_F64
+#define FL_ADJ_CTAS_F64 2
+#endif
+#ifndef FL_ADJ_CTAS_F32
+#define FL_ADJ_CTAS_F32 3
+#endif
+  static constexpr int MIN_CTAS = sizeof(T) == 8 ? FL_ADJ_CTAS_F64 : FL_ADJ_CTAS_F32;
+  // dUm, dU, dUp (stages E-F) reuse buffers dead by then: er and el (last
+  // read in stage D) and the P, V, chi-base planes (last read in stage C)
+  static_assert(NC * E <= R + 2 * D * R, "dUp must fit in the P, V and chi planes");
   static constexpr size_t smem_elems =
       (size_t)NC * R + R + 2 * D * R       // U, P, V, chi bases
       + E                                   // chi_v of evolve cells
       + 4 * NC * E                          // er, el, er_b, el_b
-      + 3 * NC * E                          // dUm, dU, dUp
       + NC * E;                             // lam_out on evolve cells
   static constexpr size_t smem_bytes = sizeof(T) * smem_elems + 64;
   __host__ __device__ static constexpr int rstride(int d) { return d == 0 ? 1 : R0; }
@@ -72,7 +83,7 @@ struct AdjGeom {
 };
 
 template <typename T, int D, int S, int FLUX>
-__global__ void __launch_bounds__(AdjGeom<T, D, S>::THREADS)
+__global__ void __launch_bounds__(AdjGeom<T, D, S>::THREADS, AdjGeom<T, D, S>::MIN_CTAS)
 adjoint_sweep_kernel(AdjointParams p) {
   using G = AdjGeom<T, D, S>;
   constexpr int NC = G::NC;
@@ -93,10 +104,10 @@ adjoint_sweep_kernel(AdjointParams p) {
   T* sEL = sER + NC * G::E;
   T* sERb = sEL + NC * G::E;
   T* sELb = sERb + NC * G::E;
-  T* sDm = sELb + NC * G::E;
-  T* sD0 = sDm + NC * G::E;
-  T* sDp = sD0 + NC * G::E;
-  T* sLam = sDp + NC * G::E;      // lam_out at evolve cells
+  T* sLam = sELb + NC * G::E;     // lam_out at evolve cells
+  T* sDm = sER;                   // stages E-F: er, el and P/V/chi are dead
+  T* sD0 = sEL;
+  T* sDp = sP;
 
   const T* __restrict__ u_in = static_cast<const T*>(p.u);
   const T* __restrict__ lo = static_cast<const T*>(p.lam_out);
