@@ -350,6 +350,8 @@ def run_ours(a, world, rank, local):
             if (dt_, fx) == (a.dtype, a.flux):
                 continue
             variants[f"{fx}_{dt_}"] = measure_variant(a, dt_, fx, states)
+        for dt_ in ("f64", "f32"):
+            variants[f"3d_hllc_{dt_}"] = measure_3d(dt_)
 
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
@@ -417,6 +419,43 @@ def measure_variant(a, dtype, flux, states, runs=3):
     cells = a.size * a.size
     return {"cell_updates_per_s": cells * T * runs / (total / 1e3),
             "sweep_gbs": 2 * 4 * elem * cells / sweep_s / 1e9, "steps_completed": it}
+
+
+def measure_3d(dtype, flux="hllc", n=256, steps=20, runs=3):
+    """3-D octant Riemann problem n^3 (the config's 3-D variant): steps HLLC /
+    van Leer MUSCL-Hancock steps at CFL 0.8 through the tile kernel, 3 sweeps a
+    step.  Reports cell-updates/s and each sweep's algorithmic bytes (one read
+    and one write of the 5-component state) against the measured HBM peak."""
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    s = SplitSolver((n, n, n), dtype=dtype, flux=flux, gamma=GAMMA)
+    x = s.new_state()
+    y = s.new_state()
+    sim = Simulation(s)
+    st = riemann_states(SEED, 3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for k in range(runs + 1):
+        s.fill_riemann(st, out=x)
+        sim.begin(x, y, 0.8, 1.0 / n, 1e30, steps)
+        e0.record()
+        sim.steps(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        if k > 0:
+            total += e0.elapsed_time(e1)
+    it, _, _, _ = sim.status()
+    elem = 8 if dtype == "f64" else 4
+    cells = n ** 3
+    sweep_s = total / 1e3 / (runs * 3 * steps)
+    gbs = 2 * 5 * elem * cells / sweep_s / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    return {"workload": f"3-D octant Riemann problem {n}^3, {steps} steps, {flux.upper()}",
+            "cell_updates_per_s": cells * steps * runs / (total / 1e3), "sweep_gbs": gbs,
+            "frac_of_measured_hbm": gbs / peak, "steps_completed": it}
 
 
 def measure_batched(seed=3, steps=200, baseline_every=4):

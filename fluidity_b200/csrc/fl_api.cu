@@ -295,6 +295,7 @@ struct fl_sim {
   int external;            // 1: the host reduces the wavespeed word and calls fl_sim_finalize
   unsigned long long* ws_word;  // external: the caller's device word (else ctrl->ws_bits)
   int cursor;              // next sweep of the current step (fl_sim_sweep)
+  void* scratch;           // 3-D: the walk's chi plane (else nullptr)
 };
 
 using namespace fl;
@@ -331,7 +332,19 @@ int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
     if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
     p.ws_accum = reinterpret_cast<unsigned long long*>(max_ws_out);
   }
+  // 3-D: the walk's chi plane, from the stream-ordered pool for this call
+  void* scratch = nullptr;
+  if (grid->dims == 3) {
+    const size_t bytes = (size_t)(grid->n[0] * grid->n[1] * grid->n[2]) * elem_size(pol);
+    cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep: scratch");
+    p.scratch = scratch;
+  }
   cudaError_t e = launch_sweep(p, pol, grid->dims, dim, st);
+  if (scratch != nullptr) {
+    const cudaError_t f = cudaFreeAsync(scratch, st);
+    if (e == cudaSuccess) e = f;
+  }
   if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
   return kOk;
 }
@@ -462,6 +475,16 @@ int fl_sim_create(fl_sim** sim, const fl_grid* grid, double gamma, uint32_t poli
     delete s;
     return fail(kENoMem, "cudaMalloc of the control block failed: %s", cudaGetErrorString(e));
   }
+  if (grid->dims == 3) {
+    const size_t bytes = (size_t)(grid->n[0] * grid->n[1] * grid->n[2]) * elem_size(s->pol);
+    e = cudaMalloc(&s->scratch, bytes);
+    if (e != cudaSuccess) {
+      cudaFree(s->ctrl);
+      delete s;
+      return fail(kENoMem, "cudaMalloc of the 3-D scratch plane failed: %s",
+                  cudaGetErrorString(e));
+    }
+  }
   e = cudaMemset(s->ctrl, 0, sizeof(StepControl));
   if (e != cudaSuccess) {
     cudaFree(s->ctrl);
@@ -474,6 +497,7 @@ int fl_sim_create(fl_sim** sim, const fl_grid* grid, double gamma, uint32_t poli
 
 int fl_sim_destroy(fl_sim* sim) {
   if (sim == nullptr) return kOk;
+  if (sim->scratch != nullptr) cudaFree(sim->scratch);
   cudaError_t e = cudaFree(sim->ctrl);
   delete sim;
   if (e != cudaSuccess) return cuda_fail(e, "fl_sim_destroy");
@@ -530,6 +554,7 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
   p.ctrl = sim->ctrl;
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;
+  p.scratch = sim->scratch;
   for (int64_t k = 0; k < nsteps; ++k) {
     // input of this step: for even D the state returns to buffer a every
     // step; for odd D it alternates a, b, a, ...
@@ -605,6 +630,7 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   p.ctrl = sim->ctrl;
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;
+  p.scratch = sim->scratch;
   p.in = si;
   p.out = so;
   const bool last = (dim == D - 1);

@@ -48,6 +48,9 @@ struct SweepParams {
   // max wavespeed: [ws_lo, ws_hi); every row when ws_hi <= ws_lo.  A slab
   // of a decomposed grid counts its own rows, not its ghost rows.
   int64_t ws_lo, ws_hi;
+  // nullable: a plane of cell-count values of the sweep's type, scratch for
+  // the 3-D walk (without it 3-D sweeps take the tile kernel)
+  void* scratch;
 };
 
 __host__ __device__ __forceinline__ bool ws_row_counts(const SweepParams& p, int64_t row) {
