@@ -61,8 +61,10 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-mm", action="store_true")
     p.add_argument("--mm-steps", type=int, default=500)
-    p.add_argument("--only", choices=["mm", "adjoint", "batched"], default=None,
+    p.add_argument("--only", choices=["mm", "adjoint", "batched", "3d"], default=None,
                    help="run one secondary workload alone (profiling); prints its own line")
+    p.add_argument("--size-3d", type=int, default=256, help="--only 3d: cells per side")
+    p.add_argument("--steps-3d", type=int, default=20, help="--only 3d: time steps per run")
     return p.parse_args()
 
 
@@ -822,6 +824,8 @@ def run_section(a, local):
         res = measure_multimaterial(steps=a.mm_steps, cpu=not a.no_cpu_baseline)
     elif a.only == "adjoint":
         res = measure_adjoint()
+    elif a.only == "3d":
+        res = {dt: measure_3d(dt, n=a.size_3d, steps=a.steps_3d) for dt in ("f64", "f32")}
     else:
         res = measure_batched()
     print(json.dumps({"section": a.only, **res}), flush=True)

@@ -35,7 +35,7 @@ namespace fl {
 #define FL_WALK3_CTAS_F64 3
 #endif
 #ifndef FL_WALK3_CTAS_F32
-#define FL_WALK3_CTAS_F32 5
+#define FL_WALK3_CTAS_F32 4
 #endif
 
 template <typename T, int S>
