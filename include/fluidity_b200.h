@@ -95,7 +95,11 @@ int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy);
  * max_ws_out (nullable, device pointer) receives the maximum wavespeed
  * max_d |u_d| + a of the OUTPUT state -- the fused form of set_wavespeeds +
  * max_element (simulator/cuda/wavespeed_initialization.cuh:85-97,
- * algorithm/max_element.hpp:28-38) for the next step. */
+ * algorithm/max_element.hpp:28-38) for the next step.
+ * 3-D grids take one cell-count plane of scratch from the device's
+ * stream-ordered pool (cudaMallocAsync on `stream`) for the call; fl_sim_*
+ * allocate theirs once at fl_sim_create, and fl_simulate_noalloc uses none
+ * (its 3-D sweeps take the shared-memory tile kernel). */
 int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out,
                    double gamma, double dtdh, uint32_t policy,
                    uint32_t boundary_mask, double* max_ws_out, void* stream);
