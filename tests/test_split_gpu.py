@@ -213,6 +213,29 @@ def test_policy_sweeps(cuda, oracle, shape, dtype, pol):
             assert err(out, ref, dtype) < TOL[dtype], (dim, reflect)
 
 
+@pytest.mark.parametrize("shape", [(4, 5, 6), (33, 4, 7), (7, 9, 70), (26, 26, 5)],
+                         ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_3d_walk_shapes(cuda, oracle, shape, dtype):
+    """The 3-D walk at the minimum extent (4), at extents that split a warp's
+    columns or a strip's rows unevenly, and with reflective ends in every
+    dimension; each sweep with its fused wavespeed against the oracle."""
+    npdt = NPDT[dtype]
+    u = oracle.prim_to_cons(random_prim(shape, 50 + shape[0], smooth=True, mild=True),
+                            GAMMA).astype(npdt)
+    ws = float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+    dtdh = npdt(0.5 / ws)
+    for reflect in (0, 7):
+        for dim in range(3):
+            ref = oracle.sweep(shape, dim, u, npdt(GAMMA), dtdh, reflect=reflect)
+            out, got_ws = gpu_sweep(shape, dim, u, float(dtdh), dtype=dtype, reflect=reflect,
+                                    want_ws=True)
+            assert err(out, ref, dtype) < TOL[dtype], (dim, reflect)
+            # the fused maximum against the oracle's maximum of the same output
+            ref_ws = float(oracle.max_wavespeed(shape, out.astype(npdt), npdt(GAMMA)))
+            assert abs(got_ws - ref_ws) <= (1e-14 if dtype == "f64" else 1e-6) * ref_ws
+
+
 def test_flattening_active_parity(cuda, oracle):
     """A compressive front smeared over a few cells (a sharp jump has one zero
     one-sided difference, so the limiter already kills its slope), oblique so

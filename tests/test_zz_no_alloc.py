@@ -47,8 +47,12 @@ def _run_noalloc(lib, capi, grid, policy, a, b, cfl, res, sim_time, steps):
     return out.value, it.value, rt.value
 
 
-@pytest.mark.parametrize("shape,states_seed", [((400,), 0), ((96, 80), 11)])
+@pytest.mark.parametrize("shape,states_seed", [((400,), 0), ((96, 80), 11), ((24, 20, 18), 5)])
 def test_noalloc_matches_allocating_loop_twice(shape, states_seed):
+    """In 3-D the allocating loop takes the register walk and the no-alloc
+    loop the tile kernel, whose fast forms round differently: there the run
+    times agree to 1e-12 and the states to 1e-10 (17 steps of rounding
+    differences) instead of bit for bit."""
     import torch
     from fluidity_b200 import build, capi
     from fluidity_b200.solver import SplitSolver
@@ -69,14 +73,17 @@ def test_noalloc_matches_allocating_loop_twice(shape, states_seed):
         a, b = s.fill_riemann(states), s.new_state()
         ptr, it, rt = _run_noalloc(lib, capi, s.grid, s.policy, a, b, 0.8, res, 1e30, steps)
         got = (a if ptr == a.data_ptr() else b).cpu().numpy()
+        exact = len(shape) < 3
         if steps == 17:
-            assert it == ref_it == 17 and rt == ref_rt
-            assert rel_err(got, ref) < 1e-12
+            assert it == ref_it == 17
+            assert rt == ref_rt if exact else abs(rt - ref_rt) <= 1e-12 * ref_rt
+            assert rel_err(got, ref) < (1e-12 if exact else 1e-10)
         else:
             ra2, rb2 = s.fill_riemann(states), s.new_state()
             p2, it2, rt2 = _run_allocating(lib, capi, s.grid, s.policy, ra2, rb2, 0.8, res,
                                            1e30, steps)
             ref2 = (ra2 if p2 == ra2.data_ptr() else rb2).cpu().numpy()
-            assert it == it2 == 9 and rt == rt2
-            assert rel_err(got, ref2) < 1e-12
+            assert it == it2 == 9
+            assert rt == rt2 if exact else abs(rt - rt2) <= 1e-12 * rt2
+            assert rel_err(got, ref2) < (1e-12 if exact else 1e-10)
     torch.cuda.synchronize()
