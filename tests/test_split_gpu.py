@@ -236,6 +236,28 @@ def test_3d_walk_shapes(cuda, oracle, shape, dtype):
             assert abs(got_ws - ref_ws) <= (1e-14 if dtype == "f64" else 1e-6) * ref_ws
 
 
+@pytest.mark.parametrize("shape", [(100001,), (317, 211), (37, 29, 23)],
+                         ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("where", ["first", "middle", "last"])
+def test_max_wavespeed_odd_sizes(cuda, oracle, shape, where):
+    """The CFL maximum (the reference's set_wavespeeds + max_element,
+    algorithm_tests_device.cu:42-77 tests its reduce on 100001 values) over
+    sizes that fill no block evenly, with the largest wavespeed planted at the
+    first, a middle or the last cell."""
+    from fluidity_b200.solver import SplitSolver
+    D = len(shape)
+    cells = int(np.prod(shape))
+    prim = random_prim(shape, 60 + D, smooth=True, mild=True)   # wavespeeds below 5
+    k = {"first": 0, "middle": cells // 2 + 7, "last": cells - 1}[where]
+    prim[2:, k] = 40.0                         # the fastest cell
+    u = oracle.prim_to_cons(prim, GAMMA)
+    s = SplitSolver(shape, gamma=GAMMA)
+    ws = s.max_wavespeed(to_dev(u, "f64")).item()
+    ref = float(oracle.max_wavespeed(shape, u, GAMMA))
+    assert abs(ws - ref) <= 1e-14 * ref
+    assert ref > 40.0                          # max_d |u_d| + a of the planted cell
+
+
 def test_flattening_active_parity(cuda, oracle):
     """A compressive front smeared over a few cells (a sharp jump has one zero
     one-sided difference, so the limiter already kills its slope), oblique so
