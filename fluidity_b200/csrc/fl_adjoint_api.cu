@@ -171,6 +171,7 @@ struct fl_adj {
   double* d_dtdh = nullptr;
   std::vector<double> dtdh;
   bool have_forward = false;
+  int64_t walk_launches = 0;  // forward sweeps launched: the strip counters' parity
 };
 
 namespace {
@@ -221,6 +222,7 @@ int fl_adj_create(fl_adj** out, const fl_grid* grid, double gamma, uint32_t poli
   if (e == cudaSuccess) e = cudaMalloc(&a->seg, a->state_bytes * grid->dims * interval);
   if (e == cudaSuccess) e = cudaMalloc(&a->work, a->state_bytes * 4);
   if (e == cudaSuccess) e = cudaMalloc(&a->ctrl, sizeof(StepControl));
+  if (e == cudaSuccess) e = cudaMemset(a->ctrl, 0, sizeof(StepControl));  // strip counters at 0
   if (e == cudaSuccess) e = cudaMalloc(&a->d_dtdh, sizeof(double) * nsteps);
   if (e != cudaSuccess) {
     fl_adj_destroy(a);
@@ -291,6 +293,8 @@ int fl_adj_forward(fl_adj* a, const void* u0, void* u_final, double cfl, double 
     for (int d = 0; d < D && e == cudaSuccess; ++d) {
       p.in = cur;
       p.out = nxt;
+      p.walk_next = a->ctrl->walk_next;
+      p.walk_slot = (int)(a->walk_launches++ & 1);
       const bool last = (d == D - 1);
       p.ws_accum = (record && last) ? &a->ctrl->ws_bits : nullptr;
       p.finalize = (record && last) ? 1 : 0;
@@ -352,6 +356,8 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
         if (last) break;  // the final output of the segment is not needed
         p.in = state_at(a->seg, sb, slot);
         p.out = state_at(a->seg, sb, slot + 1);
+        p.walk_next = a->ctrl->walk_next;
+        p.walk_slot = (int)(a->walk_launches++ & 1);
         e = fwd_sweep(g, a->policy, p, d, st);
       }
     }

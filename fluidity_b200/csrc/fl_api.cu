@@ -273,6 +273,8 @@ __global__ void init_control_kernel(StepControl* c, double cfl, double res, doub
     c->done = 0;
     c->is_f32 = is_f32;
     c->status = 0;
+    c->walk_next[0] = 0u;
+    c->walk_next[1] = 0u;
   }
 }
 
@@ -564,6 +566,8 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
     for (int d = 0; d < D; ++d) {
       p.in = si;
       p.out = so;
+      p.walk_next = sim->ctrl->walk_next;
+      p.walk_slot = (int)((sim->enqueued * D + d) & 1);
       const bool last = (d == D - 1);
       p.ws_accum = last ? &sim->ctrl->ws_bits : nullptr;
       p.finalize = last ? 1 : 0;
@@ -631,6 +635,8 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;
   p.scratch = sim->scratch;
+  p.walk_next = sim->ctrl->walk_next;
+  p.walk_slot = (int)((sim->enqueued * D + dim) & 1);
   p.in = si;
   p.out = so;
   const bool last = (dim == D - 1);

@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(256) batch_init_kernel(BatchArgs a, int nprob,
     c.ws_bits = 0ull;
     c.arrive = 0u;
     c.status = 0;
-    c.pad_ = 0;
+    c.walk_next[0] = 0u;
+    c.walk_next[1] = 0u;
     advance_control(c, m, false);
     a.ctrl[pid] = c;
   }

@@ -25,7 +25,9 @@ struct StepControl {
   int done;                    // 1 once the loop condition fails
   int is_f32;                  // round dt, dtdh and run_time through float
   int status;                  // 0, or FL_ENAN when a wavespeed was not finite
-  int pad_;
+  // strip counters of the dynamically scheduled walks, one per sweep
+  // parity: a sweep takes strips from walk_next[slot] and clears the other
+  unsigned int walk_next[2];
 };
 
 // Parameters of one dimensional sweep.
@@ -51,6 +53,11 @@ struct SweepParams {
   // nullable: a plane of cell-count values of the sweep's type, scratch for
   // the 3-D walk (without it 3-D sweeps take the tile kernel)
   void* scratch;
+  // nullable: two strip counters (StepControl::walk_next or the like); with
+  // them the walk schedules its strips dynamically, taking them from
+  // walk_next[walk_slot] and clearing the other counter for the next sweep
+  unsigned int* walk_next;
+  int walk_slot;
 };
 
 __host__ __device__ __forceinline__ bool ws_row_counts(const SweepParams& p, int64_t row) {

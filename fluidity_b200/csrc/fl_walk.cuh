@@ -263,18 +263,42 @@ __device__ __forceinline__ double cta_max(double v, double* s_red) {
   return m;
 }
 
+// Strips are scheduled statically (blockIdx.x the column group, blockIdx.y
+// and the warp the strip) or, given strip counters, dynamically: a grid of
+// resident CTAs whose warps take strips, column group fastest, from
+// walk_next[walk_slot] until none is left, so that no SM idles while a last
+// partial wave of CTAs runs.  The sweep clears the other counter, which the
+// next sweep of the stream uses.
 template <typename T, int S, int FLUX>
 __global__ void __launch_bounds__(WalkCfg<T, S>::THREADS, WalkCfg<T, S>::MIN_CTAS)
 walk_kernel_2d(SweepParams p) {
   using W = WalkCfg<T, S>;
+  // cleared before the early exit too, so that a finished run keeps both
+  // counters ready for the next sweeps on the same control block
+  if (p.walk_next != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
+    p.walk_next[1 - p.walk_slot] = 0u;
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
   const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
   __shared__ double s_red[W::WARPS];
   const int warp = threadIdx.x >> 5;
-  const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
   double ws_local = 0.0;
   const bool want_ws = (p.ws_accum != nullptr);
-  walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0, W::RY, ws_local, want_ws);
+  if (p.walk_next == nullptr) {
+    const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
+    walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0, W::RY, ws_local, want_ws);
+  } else {
+    const int64_t ncol = (p.n[0] + W::OWN - 1) / W::OWN;
+    const int64_t items = ncol * ((p.n[1] + W::RY - 1) / W::RY);
+    unsigned int* next = &p.walk_next[p.walk_slot];
+    for (;;) {
+      unsigned int item = 0u;
+      if ((threadIdx.x & 31) == 0) item = atomicAdd(next, 1u);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if ((int64_t)item >= items) break;
+      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)item % ncol, ((int64_t)item / ncol) * W::RY,
+                                W::RY, ws_local, want_ws);
+    }
+  }
   if (want_ws) {
     const double m = cta_max<W::WARPS>(ws_local, s_red);
     if (threadIdx.x == 0) {
