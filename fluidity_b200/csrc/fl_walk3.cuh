@@ -236,16 +236,36 @@ template <typename T, int S, int FLUX>
 __global__ void __launch_bounds__(Walk3Cfg<T, S>::THREADS, Walk3Cfg<T, S>::MIN_CTAS)
 walk_kernel_3d(SweepParams p, const T* __restrict__ xc) {
   using W = Walk3Cfg<T, S>;
+  if (p.walk_next != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
+    p.walk_next[1 - p.walk_slot] = 0u;
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
   const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
   __shared__ double s_red[W::WARPS];
   const int warp = threadIdx.x >> 5;
-  const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
   double ws_local = 0.0;
   const bool want_ws = (p.ws_accum != nullptr);
-  for (int64_t pl = blockIdx.z; pl < p.n[W::DT]; pl += gridDim.z)
-    walk_strip_3d<T, S, FLUX>(p, xc, dtdh, (int64_t)blockIdx.x, y0, W::RY, pl, ws_local,
-                              want_ws);
+  if (p.walk_next == nullptr) {
+    const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
+    for (int64_t pl = blockIdx.z; pl < p.n[W::DT]; pl += gridDim.z)
+      walk_strip_3d<T, S, FLUX>(p, xc, dtdh, (int64_t)blockIdx.x, y0, W::RY, pl, ws_local,
+                                want_ws);
+  } else {
+    // strips taken dynamically, column group fastest, then the strip along
+    // the row dimension, then the plane
+    const int64_t ncol = (p.n[0] + W::OWN - 1) / W::OWN;
+    const int64_t nrow = (p.n[W::DR] + W::RY - 1) / W::RY;
+    const int64_t items = ncol * nrow * p.n[W::DT];
+    unsigned int* next = &p.walk_next[p.walk_slot];
+    for (;;) {
+      unsigned int item = 0u;
+      if ((threadIdx.x & 31) == 0) item = atomicAdd(next, 1u);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if ((int64_t)item >= items) break;
+      const int64_t cr = (int64_t)item % (ncol * nrow);
+      walk_strip_3d<T, S, FLUX>(p, xc, dtdh, cr % ncol, (cr / ncol) * W::RY, W::RY,
+                                (int64_t)item / (ncol * nrow), ws_local, want_ws);
+    }
+  }
   if (want_ws) {
     const double m = cta_max<W::WARPS>(ws_local, s_red);
     if (threadIdx.x == 0) {
