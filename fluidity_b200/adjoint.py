@@ -22,7 +22,7 @@ class Adjoint:
     """Checkpointed forward / backward of nsteps steps on one grid."""
 
     def __init__(self, shape, nsteps, dtype="f64", flux="hllc", gamma=1.4, boundary_mask=0,
-                 interval=0, flatten=True, recon="muscl"):
+                 interval=0, flatten=True, recon="muscl", p_inf=0.0):
         self.lib = capi.load()
         self.shape = tuple(int(v) for v in shape)
         self.nsteps = int(nsteps)
@@ -35,6 +35,10 @@ class Adjoint:
                                           self.policy, int(boundary_mask), self.nsteps,
                                           int(interval)), self.lib)
         self.handle = h
+        self.p_inf = float(p_inf)
+        if self.p_inf != 0.0:
+            mat = capi.Material(self.gamma, self.p_inf)
+            capi.check(self.lib.fl_adj_set_material(h, C.byref(mat)), self.lib)
 
     def __del__(self):
         h = getattr(self, "handle", None)

@@ -144,7 +144,10 @@ PROTOTYPES = {
                                    C.c_uint32, _P]),
     "fl_adj_create": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,
                                 C.c_int64, C.c_int64]),
+    "fl_adjoint_sweep_mat": (C.c_int, [_G, C.c_int, _P, _P, _P, C.POINTER(Material), C.c_double,
+                                       C.c_uint32, C.c_uint32, _P]),
     "fl_adj_destroy": (C.c_int, [_P]),
+    "fl_adj_set_material": (C.c_int, [_P, C.POINTER(Material)]),
     "fl_adj_forward": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.POINTER(C.c_double), _P]),
     "fl_adj_dtdh": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "fl_adj_backward": (C.c_int, [_P, _P, _P, _P]),

@@ -92,10 +92,11 @@ FL_HD void flux_rev(const Cons<T, D>& u, const Derived<T, D>& q, int d, T gm1,
 template <typename T, int D>
 FL_HD void hllc_rev(const Cons<T, D>& ul, const Derived<T, D>& ql, const Cons<T, D>& ur,
                     const Derived<T, D>& qr, int d, T gamma, T gm1, T adi, const Cons<T, D>& g,
-                    Cons<T, D>& ubl, Cons<T, D>& ubr) {
+                    Cons<T, D>& ubl, Cons<T, D>& ubr, T pinf = T(0)) {
   const T pl = ql.p, pr = qr.p, vl = ql.v[d], vr = qr.v[d];
-  const T al = fl_sqrt<T>(gamma * pl * ql.rinv);
-  const T ar = fl_sqrt<T>(gamma * pr * qr.rinv);
+  // sound speeds from p + p_inf (p_inf = 0: the ideal gas)
+  const T al = fl_sqrt<T>(gamma * (pl + pinf) * ql.rinv);
+  const T ar = fl_sqrt<T>(gamma * (pr + pinf) * qr.rinv);
   const T A1 = vr - vl, A2 = ur.v[0] + ul.v[0], A3 = al + ar;
   const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * A1 * A2 * A3));
   const T p_star = std_max(T(0), p_pvrs);
@@ -232,16 +233,16 @@ FL_HD void hllc_rev(const Cons<T, D>& ul, const Derived<T, D>& ql, const Cons<T,
   ubl.v[0] += A2b;
   alb += A3b;
   arb += A3b;
-  // a = sqrt(gamma p r)
+  // a = sqrt(gamma (p + p_inf) r)
   if (al > T(0)) {
     const T Ab = alb / (T(2) * al);
     plb += Ab * gamma * ql.rinv;
-    bl.r += Ab * gamma * pl;
+    bl.r += Ab * gamma * (pl + pinf);
   }
   if (ar > T(0)) {
     const T Ab = arb / (T(2) * ar);
     prb += Ab * gamma * qr.rinv;
-    br.r += Ab * gamma * pr;
+    br.r += Ab * gamma * (pr + pinf);
   }
   bl.p += plb;
   br.p += prb;
@@ -290,12 +291,13 @@ FL_HD void force_rev(const Cons<T, D>& ul, const Derived<T, D>& ql, const Cons<T
 
 template <int FLUX, typename T, int D>
 FL_HD void riemann_rev(const Cons<T, D>& ul, const Cons<T, D>& ur, int d, T gamma, T gm1,
-                       T adi, T dtdh, const Cons<T, D>& g, Cons<T, D>& ubl, Cons<T, D>& ubr) {
+                       T adi, T dtdh, const Cons<T, D>& g, Cons<T, D>& ubl, Cons<T, D>& ubr,
+                       T pinf = T(0)) {
   const Derived<T, D> ql = derive(ul, gm1), qr = derive(ur, gm1);
   if constexpr (FLUX == kForce) {
     force_rev(ul, ql, ur, qr, d, gm1, dtdh, g, ubl, ubr);
   } else {
-    hllc_rev(ul, ql, ur, qr, d, gamma, gm1, adi, g, ubl, ubr);
+    hllc_rev(ul, ql, ur, qr, d, gamma, gm1, adi, g, ubl, ubr, pinf);
   }
 }
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -83,13 +84,22 @@ int check_adj_args(const fl_grid* g, uint32_t policy, uint32_t boundary_mask, do
   return kOk;
 }
 
-AdjointParams make_adj_params(const fl_grid* g, uint32_t policy, double gamma, double dtdh,
-                              uint32_t boundary) {
+int check_adj_material(const fl_material* m) {
+  if (m == nullptr) return set_error(kEInval, "material is NULL");
+  if (!(m->gamma > 1.0)) return set_error(kEInval, "gamma must exceed 1");
+  if (!(m->p_inf >= 0.0) || m->p_inf > DBL_MAX)
+    return set_error(kEInval, "p_inf must be finite and >= 0");
+  return kOk;
+}
+
+AdjointParams make_adj_params(const fl_grid* g, uint32_t policy, double gamma, double pinf,
+                              double dtdh, uint32_t boundary) {
   AdjointParams p;
   memset(&p, 0, sizeof(p));
   p.pitch = g->pitch;
   for (int d = 0; d < 3; ++d) p.n[d] = g->n[d];
   p.gamma = gamma;
+  p.pinf = pinf;
   p.dtdh = dtdh;
   p.basic = (int)((policy >> 4) & 1u);
   p.flatten = ((policy >> 5) & 1u) ? 0 : 1;
@@ -97,13 +107,14 @@ AdjointParams make_adj_params(const fl_grid* g, uint32_t policy, double gamma, d
   return p;
 }
 
-SweepParams make_fwd_params(const fl_grid* g, uint32_t policy, double gamma, double dtdh,
-                            uint32_t boundary) {
+SweepParams make_fwd_params(const fl_grid* g, uint32_t policy, double gamma, double pinf,
+                            double dtdh, uint32_t boundary) {
   SweepParams p;
   memset(&p, 0, sizeof(p));
   p.pitch = g->pitch;
   for (int d = 0; d < 3; ++d) p.n[d] = g->n[d];
   p.gamma = gamma;
+  p.pinf = pinf;
   p.dtdh = dtdh;
   p.limiter = (int)((policy >> 3) & 1u);
   p.basic = (int)((policy >> 4) & 1u);
@@ -135,8 +146,8 @@ __global__ void adj_init_control_kernel(StepControl* c, double cfl, double res, 
   }
 }
 
-template <typename T, int D>
-__global__ void adj_wavespeed_kernel(const T* in, int64_t pitch, int64_t cells, T gamma,
+template <typename T, int D, bool STIFF>
+__global__ void adj_wavespeed_kernel(const T* in, int64_t pitch, int64_t cells, T gamma, T pinf,
                                      StepControl* ctrl) {
   __shared__ double s_red[8];
   const T gm1 = gamma - T(1);
@@ -146,7 +157,7 @@ __global__ void adj_wavespeed_kernel(const T* in, int64_t pitch, int64_t cells, 
     Cons<T, D> u;
 #pragma unroll
     for (int c = 0; c < D + 2; ++c) u.v[c] = in[c * pitch + i];
-    ws_max(local, (double)max_wavespeed_q(derive(u, gm1), gamma));
+    ws_max(local, (double)max_wavespeed_q<STIFF>(derive(u, gm1), gamma, pinf));
   }
   cta_wavespeed_commit<256>(local, &ctrl->ws_bits, ctrl, 1, false, s_red);
 }
@@ -161,6 +172,7 @@ struct fl_adj {
   uint32_t policy;
   uint32_t boundary;
   double gamma;
+  double pinf = 0.0;        // stiffened fluid's p_inf; 0 for the ideal gas
   int64_t nsteps;
   int64_t interval;
   size_t state_bytes;
@@ -182,15 +194,18 @@ void* state_at(char* base, size_t bytes, int64_t i) { return base + (size_t)i * 
 
 extern "C" {
 
-int fl_adjoint_sweep(const fl_grid* grid, int dim, const void* u_in, const void* lambda_out,
-                     void* lambda_in, double gamma, double dtdh, uint32_t policy,
-                     uint32_t boundary_mask, void* stream) {
-  int rc = check_adj_args(grid, policy, boundary_mask, gamma);
+int fl_adjoint_sweep_mat(const fl_grid* grid, int dim, const void* u_in,
+                         const void* lambda_out, void* lambda_in, const fl_material* mat,
+                         double dtdh, uint32_t policy, uint32_t boundary_mask, void* stream) {
+  int rc = check_adj_material(mat);
+  if (rc) return rc;
+  const double gamma = mat->gamma;
+  rc = check_adj_args(grid, policy, boundary_mask, gamma);
   if (rc) return rc;
   if (dim < 0 || dim >= grid->dims) return set_error(kEInval, "dim %d out of range", dim);
   if (!u_in || !lambda_out || !lambda_in) return set_error(kEInval, "NULL buffer");
   if (lambda_in == lambda_out) return set_error(kEInval, "lambda_in and lambda_out must differ");
-  AdjointParams p = make_adj_params(grid, policy, gamma, dtdh, boundary_mask);
+  AdjointParams p = make_adj_params(grid, policy, gamma, mat->p_inf, dtdh, boundary_mask);
   p.u = u_in;
   p.lam_out = lambda_out;
   p.lam_in = lambda_in;
@@ -198,6 +213,14 @@ int fl_adjoint_sweep(const fl_grid* grid, int dim, const void* u_in, const void*
                              static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return set_error(kECuda, "fl_adjoint_sweep: %s", cudaGetErrorString(e));
   return kOk;
+}
+
+int fl_adjoint_sweep(const fl_grid* grid, int dim, const void* u_in, const void* lambda_out,
+                     void* lambda_in, double gamma, double dtdh, uint32_t policy,
+                     uint32_t boundary_mask, void* stream) {
+  const fl_material mat{gamma, 0.0};
+  return fl_adjoint_sweep_mat(grid, dim, u_in, lambda_out, lambda_in, &mat, dtdh, policy,
+                              boundary_mask, stream);
 }
 
 int fl_adj_create(fl_adj** out, const fl_grid* grid, double gamma, uint32_t policy,
@@ -233,6 +256,16 @@ int fl_adj_create(fl_adj** out, const fl_grid* grid, double gamma, uint32_t poli
   return kOk;
 }
 
+int fl_adj_set_material(fl_adj* a, const fl_material* mat) {
+  if (a == nullptr) return set_error(kEInval, "adjoint handle is NULL");
+  int rc = check_adj_material(mat);
+  if (rc) return rc;
+  a->gamma = mat->gamma;
+  a->pinf = mat->p_inf;
+  a->have_forward = false;  // a recorded forward pass belongs to the old material
+  return kOk;
+}
+
 int fl_adj_destroy(fl_adj* a) {
   if (a == nullptr) return kOk;
   cudaFree(a->ckpt);
@@ -261,20 +294,34 @@ int fl_adj_forward(fl_adj* a, const void* u0, void* u_final, double cfl, double 
                                               (a->policy & 1u) ? 1 : 0);
     const int64_t cells = g->n[0] * g->n[1] * g->n[2];
     const unsigned blocks = (unsigned)std::min<int64_t>((cells + 255) / 256, 148 * 8);
+    const bool f32 = (a->policy & 1u) != 0;
+    const bool stiff = a->pinf != 0.0;
     if (D == 1) {
-      if (a->policy & 1u)
-        adj_wavespeed_kernel<float, 1><<<blocks, 256, 0, st>>>((const float*)cur, g->pitch, cells,
-                                                               (float)a->gamma, a->ctrl);
+      if (f32 && stiff)
+        adj_wavespeed_kernel<float, 1, true><<<blocks, 256, 0, st>>>(
+            (const float*)cur, g->pitch, cells, (float)a->gamma, (float)a->pinf, a->ctrl);
+      else if (f32)
+        adj_wavespeed_kernel<float, 1, false><<<blocks, 256, 0, st>>>(
+            (const float*)cur, g->pitch, cells, (float)a->gamma, 0.0f, a->ctrl);
+      else if (stiff)
+        adj_wavespeed_kernel<double, 1, true><<<blocks, 256, 0, st>>>(
+            (const double*)cur, g->pitch, cells, a->gamma, a->pinf, a->ctrl);
       else
-        adj_wavespeed_kernel<double, 1><<<blocks, 256, 0, st>>>((const double*)cur, g->pitch, cells,
-                                                                a->gamma, a->ctrl);
+        adj_wavespeed_kernel<double, 1, false><<<blocks, 256, 0, st>>>(
+            (const double*)cur, g->pitch, cells, a->gamma, 0.0, a->ctrl);
     } else {
-      if (a->policy & 1u)
-        adj_wavespeed_kernel<float, 2><<<blocks, 256, 0, st>>>((const float*)cur, g->pitch, cells,
-                                                               (float)a->gamma, a->ctrl);
+      if (f32 && stiff)
+        adj_wavespeed_kernel<float, 2, true><<<blocks, 256, 0, st>>>(
+            (const float*)cur, g->pitch, cells, (float)a->gamma, (float)a->pinf, a->ctrl);
+      else if (f32)
+        adj_wavespeed_kernel<float, 2, false><<<blocks, 256, 0, st>>>(
+            (const float*)cur, g->pitch, cells, (float)a->gamma, 0.0f, a->ctrl);
+      else if (stiff)
+        adj_wavespeed_kernel<double, 2, true><<<blocks, 256, 0, st>>>(
+            (const double*)cur, g->pitch, cells, a->gamma, a->pinf, a->ctrl);
       else
-        adj_wavespeed_kernel<double, 2><<<blocks, 256, 0, st>>>((const double*)cur, g->pitch, cells,
-                                                                a->gamma, a->ctrl);
+        adj_wavespeed_kernel<double, 2, false><<<blocks, 256, 0, st>>>(
+            (const double*)cur, g->pitch, cells, a->gamma, 0.0, a->ctrl);
     }
     e = cudaGetLastError();
   }
@@ -287,8 +334,8 @@ int fl_adj_forward(fl_adj* a, const void* u0, void* u_final, double cfl, double 
       record_dtdh_kernel<<<1, 32, 0, st>>>(a->ctrl, a->d_dtdh + k);
       e = cudaGetLastError();
     }
-    SweepParams p = make_fwd_params(g, a->policy, a->gamma, record ? 0.0 : frozen_dtdh[k],
-                                    a->boundary);
+    SweepParams p = make_fwd_params(g, a->policy, a->gamma, a->pinf,
+                                    record ? 0.0 : frozen_dtdh[k], a->boundary);
     if (record) p.ctrl = a->ctrl;
     for (int d = 0; d < D && e == cudaSuccess; ++d) {
       p.in = cur;
@@ -349,7 +396,7 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
     void* cur = state_at(a->seg, sb, 0);
     e = cudaMemcpyAsync(cur, state_at(a->ckpt, sb, j), sb, cudaMemcpyDeviceToDevice, st);
     for (int64_t k = k0; k < k1 && e == cudaSuccess; ++k) {
-      SweepParams p = make_fwd_params(g, a->policy, a->gamma, a->dtdh[k], a->boundary);
+      SweepParams p = make_fwd_params(g, a->policy, a->gamma, a->pinf, a->dtdh[k], a->boundary);
       for (int d = 0; d < D && e == cudaSuccess; ++d) {
         const int64_t slot = (k - k0) * D + d;
         const bool last = (k == k1 - 1) && (d == D - 1);
@@ -364,7 +411,8 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
     // adjoint sweeps in reverse order
     for (int64_t k = k1 - 1; k >= k0 && e == cudaSuccess; --k) {
       for (int d = D - 1; d >= 0 && e == cudaSuccess; --d) {
-        AdjointParams p = make_adj_params(g, a->policy, a->gamma, a->dtdh[k], a->boundary);
+        AdjointParams p =
+            make_adj_params(g, a->policy, a->gamma, a->pinf, a->dtdh[k], a->boundary);
         p.u = state_at(a->seg, sb, (k - k0) * D + d);
         p.lam_out = la;
         p.lam_in = lb;

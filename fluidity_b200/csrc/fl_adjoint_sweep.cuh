@@ -32,6 +32,7 @@ struct AdjointParams {
   int64_t pitch;
   int64_t n[3];
   double gamma;
+  double pinf;          // stiffened fluid's p_inf (0: ideal gas)
   double dtdh;
   int flatten;
   int basic;
@@ -90,6 +91,7 @@ adjoint_sweep_kernel(AdjointParams p) {
   constexpr int NT = G::THREADS;
   const T gamma = (T)p.gamma, gm1 = gamma - T(1);
   const T adi = (gamma + T(1)) / (T(2) * gamma);
+  const T pinf = (T)p.pinf;
   const T dtdh = (T)p.dtdh;
   const bool muscl = !p.basic;
   const bool flatten = muscl && p.flatten;
@@ -244,7 +246,7 @@ adjoint_sweep_kernel(AdjointParams p) {
       if constexpr (FLUX == kForce)
         riemann_rev<kForce>(ul, ur, S, gamma, gm1, adi, dtdh, g, bl, br);
       else
-        riemann_rev<kHllc>(ul, ur, S, gamma, gm1, adi, dtdh, g, bl, br);
+        riemann_rev<kHllc>(ul, ur, S, gamma, gm1, adi, dtdh, g, bl, br, pinf);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         sERb[c * G::E + el_idx] = bl.v[c];

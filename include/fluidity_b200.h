@@ -334,6 +334,12 @@ int fl_batch_tuning(const fl_batch* batch, int32_t* out, int32_t n);
 int fl_adjoint_sweep(const fl_grid* grid, int dim, const void* u_in, const void* lambda_out,
                      void* lambda_in, double gamma, double dtdh, uint32_t policy,
                      uint32_t boundary_mask, void* stream);
+/* The same for either material: the stiffened fluid's sound speed
+ * sqrt(gamma (p + p_inf) / rho) in the HLLC wave-speed estimates is
+ * differentiated with p_inf as a constant (material/stiff_fluid.hpp:92-96). */
+int fl_adjoint_sweep_mat(const fl_grid* grid, int dim, const void* u_in,
+                         const void* lambda_out, void* lambda_in, const fl_material* mat,
+                         double dtdh, uint32_t policy, uint32_t boundary_mask, void* stream);
 
 typedef struct fl_adj fl_adj;
 
@@ -342,6 +348,10 @@ typedef struct fl_adj fl_adj;
 int fl_adj_create(fl_adj** adj, const fl_grid* grid, double gamma, uint32_t policy,
                   uint32_t boundary_mask, int64_t nsteps, int64_t interval);
 int fl_adj_destroy(fl_adj* adj);
+
+/* Replaces the material given at creation (gamma and p_inf); the next
+ * backward pass needs a new forward pass. */
+int fl_adj_set_material(fl_adj* adj, const fl_material* mat);
 
 /* Forward: nsteps steps from u0 into u_final (device), storing checkpoints.
  * frozen_dtdh == NULL: CFL steps (cfl, res) computed on the device and

@@ -40,16 +40,24 @@ static C2 axpy(const C2& x, double e, const C2& d) {
 }
 
 static const double gam = 1.4, gm1 = 0.4, adi = 2.4 / 2.8;
+static const double pinf_stiff = 6.0;  // stiffened fluid: p + p_inf under the sound speed
 
 template <int FLUX>
 static C2 rs(const C2& l, const C2& r, int d, double dtdh) {
   C2 f;
-  riemann_q<FLUX>(l, derive(l, gm1), r, derive(r, gm1), d, gam, gm1, adi, dtdh, f);
+  const double pinf = (FLUX & kStiffEos) ? pinf_stiff : 0.0;
+  riemann_q<FLUX>(l, derive(l, gm1), r, derive(r, gm1), d, gam, gm1, adi, dtdh, f, pinf);
   return f;
 }
 
+// which: 0 HLLC, 1 FORCE, 2 HLLC of the stiffened fluid
+static C2 rs_which(int which, const C2& l, const C2& r, int d, double dtdh) {
+  return which == 1 ? rs<kForce>(l, r, d, dtdh)
+                    : which == 2 ? rs<kHllc | kStiffEos>(l, r, d, dtdh) : rs<kHllc>(l, r, d, dtdh);
+}
+
 int main() {
-  double worst_flux = 0, worst_hllc = 0, worst_force = 0, worst_evolve = 0;
+  double worst_flux = 0, worst_hllc = 0, worst_force = 0, worst_evolve = 0, worst_stiff = 0;
   int regions[4] = {0, 0, 0, 0};
   for (int trial = 0; trial < 4000; ++trial) {
     const C2 a = rand_state(), b = rand_state(), c3 = rand_state();
@@ -79,11 +87,9 @@ int main() {
       worst_flux = std::fmax(worst_flux, std::fabs(fd - ad) / std::fmax(std::fabs(ad), sc));
     }
     // Riemann fluxes; skip the rare draws where a branch flips within +-eps
-    for (int which = 0; which < 2; ++which) {
-      C2 fp = which ? rs<kForce>(axpy(a, eps, dl), axpy(b, eps, dr), d, dtdh)
-                    : rs<kHllc>(axpy(a, eps, dl), axpy(b, eps, dr), d, dtdh);
-      C2 fm = which ? rs<kForce>(axpy(a, -eps, dl), axpy(b, -eps, dr), d, dtdh)
-                    : rs<kHllc>(axpy(a, -eps, dl), axpy(b, -eps, dr), d, dtdh);
+    for (int which = 0; which < 3; ++which) {
+      C2 fp = rs_which(which, axpy(a, eps, dl), axpy(b, eps, dr), d, dtdh);
+      C2 fm = rs_which(which, axpy(a, -eps, dl), axpy(b, -eps, dr), d, dtdh);
       double fd = 0, sc = 0;
       for (int c = 0; c < 4; ++c) {
         fd += g.v[c] * (fp.v[c] - fm.v[c]) / (2 * eps);
@@ -92,20 +98,21 @@ int main() {
       C2 ubl, ubr;
       zero(ubl);
       zero(ubr);
-      if (which)
+      if (which == 1)
         riemann_rev<kForce>(a, b, d, gam, gm1, adi, dtdh, g, ubl, ubr);
       else
-        riemann_rev<kHllc>(a, b, d, gam, gm1, adi, dtdh, g, ubl, ubr);
+        riemann_rev<kHllc>(a, b, d, gam, gm1, adi, dtdh, g, ubl, ubr,
+                           which == 2 ? pinf_stiff : 0.0);
       const double ad = dot(ubl, dl) + dot(ubr, dr);
       const double err = std::fabs(fd - ad) / std::fmax(std::fabs(ad), sc);
-      if (which == 0) {
+      if (which != 1) {
         // classify the region for coverage
         const Derived<double, 2> ql = derive(a, gm1), qr = derive(b, gm1);
         (void)ql; (void)qr;
         if (err > 1e-4) {
           // check for a branch flip: the reverse of a piecewise function is
           // only defined inside a piece
-          C2 f0 = rs<kHllc>(a, b, d, dtdh);
+          C2 f0 = rs_which(which, a, b, d, dtdh);
           double fd1 = 0, fd2 = 0;
           for (int c = 0; c < 4; ++c) {
             fd1 += g.v[c] * (fp.v[c] - f0.v[c]) / eps;
@@ -113,7 +120,8 @@ int main() {
           }
           if (std::fabs(fd1 - fd2) > 1e-3 * (std::fabs(fd1) + 1e-8)) continue;
         }
-        worst_hllc = std::fmax(worst_hllc, err);
+        if (which == 0) worst_hllc = std::fmax(worst_hllc, err);
+        else worst_stiff = std::fmax(worst_stiff, err);
       } else {
         worst_force = std::fmax(worst_force, err);
       }
@@ -156,8 +164,9 @@ int main() {
     }
     (void)regions;
   }
-  std::printf("flux %.3e hllc %.3e force %.3e evolve %.3e\n", worst_flux, worst_hllc,
-              worst_force, worst_evolve);
+  std::printf("flux %.3e hllc %.3e stiff hllc %.3e force %.3e evolve %.3e\n", worst_flux,
+              worst_hllc, worst_stiff, worst_force, worst_evolve);
   const double tol = 1e-5;
-  return (worst_flux < tol && worst_hllc < tol && worst_force < tol && worst_evolve < tol) ? 0 : 1;
+  return (worst_flux < tol && worst_hllc < tol && worst_stiff < tol && worst_force < tol &&
+          worst_evolve < tol) ? 0 : 1;
 }

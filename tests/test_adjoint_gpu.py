@@ -227,3 +227,103 @@ def test_adjoint_1d(cuda):
     fd = torch.sum(lamN * (up - um)).item() / (2 * eps)
     ad = torch.sum(lam0 * du).item()
     assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+
+
+# ---- the stiffened fluid (p + p_inf under the sound speed) -------------------
+
+P_INF = 2.0
+
+
+@pytest.mark.parametrize("shape,dim", [((64,), 0), ((40, 24), 0), ((40, 24), 1)])
+@pytest.mark.parametrize("flux", ["hllc", "force"])
+@pytest.mark.parametrize("reflect", [0, 1])
+def test_adjoint_sweep_transpose_stiff(cuda, shape, dim, flux, reflect):
+    """fl_adjoint_sweep_mat against central differences of the stiffened
+    fluid's forward sweep (fl_split_sweep_mat), flattening off."""
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.solver import SplitSolver
+    lib = capi.load()
+    u = torch.from_numpy(_smooth_state(shape, 5 + dim)).cuda()
+    s = SplitSolver(shape, flux=flux, gamma=GAMMA, boundary_mask=reflect, flatten=False,
+                    p_inf=P_INF)
+    ws = s.max_wavespeed(u).item()
+    dtdh = 0.6 / ws
+    g = torch.Generator(device="cpu").manual_seed(13)
+    lam = torch.randn(u.shape, generator=g, dtype=torch.float64).cuda()
+    du = (torch.randn(u.shape, generator=g, dtype=torch.float64) * 1e-2).cuda() * u.abs()
+    eps = 1e-6
+    up, um = torch.empty_like(u), torch.empty_like(u)
+    s.sweep(u + eps * du, up, dim, dtdh)
+    s.sweep(u - eps * du, um, dim, dtdh)
+    fd = torch.sum(lam * (up - um)).item() / (2 * eps)
+    lam_in = torch.empty_like(u)
+    mat = capi.Material(GAMMA, P_INF)
+    capi.check(lib.fl_adjoint_sweep_mat(C.byref(s.grid), dim, C.c_void_p(u.data_ptr()),
+                                        C.c_void_p(lam.data_ptr()),
+                                        C.c_void_p(lam_in.data_ptr()), C.byref(mat), dtdh,
+                                        s.policy, reflect, None))
+    torch.cuda.synchronize()
+    ad = torch.sum(lam_in * du).item()
+    assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-12), (fd, ad)
+    if flux == "hllc":
+        # the ideal-gas adjoint is a different transpose: p_inf reaches it
+        lam_ig = torch.empty_like(u)
+        capi.check(lib.fl_adjoint_sweep(C.byref(s.grid), dim, C.c_void_p(u.data_ptr()),
+                                        C.c_void_p(lam.data_ptr()),
+                                        C.c_void_p(lam_ig.data_ptr()), GAMMA, dtdh, s.policy,
+                                        reflect, None))
+        torch.cuda.synchronize()
+        assert not torch.equal(lam_ig, lam_in)
+
+
+def test_adjoint_stiff_rollout(cuda):
+    """Checkpointed rollout of the stiffened fluid: the recorded first step is
+    the stiff CFL step, the forward pass equals fl_split_sweep_mat applied
+    with the recorded steps, and the gradient matches central differences."""
+    import torch
+    from fluidity_b200.adjoint import Adjoint
+    from fluidity_b200.solver import SplitSolver
+    shape = (128,)
+    u0 = torch.from_numpy(_smooth_state(shape, 23)).cuda()
+    adj = Adjoint(shape, 30, interval=6, flatten=False, p_inf=P_INF)
+    uN = adj.forward(u0, 0.8)
+    dts = adj.dtdh()
+    s = SplitSolver(shape, gamma=GAMMA, flatten=False, p_inf=P_INF)
+    ws = s.max_wavespeed(u0).item()
+    assert dts[0] == pytest.approx(0.8 / ws, rel=1e-14)
+    ws_ideal = SplitSolver(shape, gamma=GAMMA, flatten=False).max_wavespeed(u0).item()
+    assert ws > ws_ideal
+    cur = u0.clone()
+    for k in range(30):
+        nxt = torch.empty_like(cur)
+        s.sweep(cur, nxt, 0, float(dts[k]))
+        cur = nxt
+    torch.cuda.synchronize()
+    assert torch.equal(cur, uN)
+    g = torch.Generator(device="cpu").manual_seed(6)
+    lamN = torch.randn(uN.shape, generator=g, dtype=torch.float64).cuda()
+    lam0 = adj.backward(lamN)
+    du = (torch.randn(u0.shape, generator=g, dtype=torch.float64) * 1e-2).cuda() * u0.abs()
+    eps = 1e-6
+    up = adj.forward(u0 + eps * du, 0.8, frozen_dtdh=dts)
+    um = adj.forward(u0 - eps * du, 0.8, frozen_dtdh=dts)
+    fd = torch.sum(lamN * (up - um)).item() / (2 * eps)
+    ad = torch.sum(lam0 * du).item()
+    assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+
+
+def test_adjoint_set_material_drops_the_forward_pass(cuda):
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.adjoint import Adjoint
+    shape = (64,)
+    u0 = torch.from_numpy(_smooth_state(shape, 29)).cuda()
+    adj = Adjoint(shape, 4)
+    uN = adj.forward(u0, 0.8)
+    mat = capi.Material(GAMMA, P_INF)
+    capi.check(adj.lib.fl_adj_set_material(adj.handle, C.byref(mat)), adj.lib)
+    with pytest.raises(capi.FlError):
+        adj.backward(torch.ones_like(uN))
+    bad = capi.Material(GAMMA, -1.0)
+    assert adj.lib.fl_adj_set_material(adj.handle, C.byref(bad)) != 0
