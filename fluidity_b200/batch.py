@@ -41,7 +41,7 @@ class Batch:
     """A set of problems, their arenas and the fl_batch handle."""
 
     def __init__(self, problems, dtype: str = "f32", flux: str = "hllc", gamma: float = 1.4,
-                 boundary_mask: int = 0, device="cuda"):
+                 boundary_mask: int = 0, device="cuda", p_inf: float = 0.0):
         self.lib = capi.load()
         self.problems = problems
         self.dtype = dtype
@@ -72,6 +72,10 @@ class Batch:
         capi.check(self.lib.fl_batch_create(C.byref(h), descs, len(problems), gamma,
                                             self.policy, boundary_mask), self.lib)
         self.handle = h
+        self.p_inf = float(p_inf)
+        if self.p_inf != 0.0:
+            mat = capi.Material(float(gamma), self.p_inf)
+            capi.check(self.lib.fl_batch_set_material(h, C.byref(mat)), self.lib)
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -89,9 +93,15 @@ class Batch:
             elem = self.a.element_size()
             ptr = self.a.data_ptr() + self.offsets[i] * elem
             sp = np.ascontiguousarray(states, dtype=np.float64)
-            capi.check(self.lib.fl_fill_riemann(C.byref(g), sp.ctypes.data_as(C.c_void_p),
-                                                self.gamma, self.policy, C.c_void_p(ptr),
-                                                None), self.lib)
+            if self.p_inf != 0.0:
+                mat = capi.Material(float(self.gamma), self.p_inf)
+                rc = self.lib.fl_fill_riemann_mat(C.byref(g), sp.ctypes.data_as(C.c_void_p),
+                                                  C.byref(mat), self.policy, C.c_void_p(ptr),
+                                                  None)
+            else:
+                rc = self.lib.fl_fill_riemann(C.byref(g), sp.ctypes.data_as(C.c_void_p),
+                                              self.gamma, self.policy, C.c_void_p(ptr), None)
+            capi.check(rc, self.lib)
 
     def state(self, i, arena=None):
         arena = self.a if arena is None else arena

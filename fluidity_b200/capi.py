@@ -132,6 +132,7 @@ PROTOTYPES = {
     "fl_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(BatchDesc), C.c_int32, C.c_double,
                                   C.c_uint32, C.c_uint32]),
     "fl_batch_destroy": (C.c_int, [_P]),
+    "fl_batch_set_material": (C.c_int, [_P, C.POINTER(Material)]),
     "fl_batch_begin": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_int64, _P]),
     "fl_batch_steps": (C.c_int, [_P, C.c_int64, _P]),
     "fl_batch_capture": (C.c_int, [_P, C.c_int64]),

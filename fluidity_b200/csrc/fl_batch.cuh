@@ -55,6 +55,7 @@ struct BatchArgs {
   void* arena_a;              // states; every problem's result ends here
   void* arena_b;              // 2-D ping-pong partner
   double gamma;
+  double pinf;                // stiffened fluid's p_inf (0: ideal gas), every problem
   int limiter;
   int basic;
   int flatten;
@@ -102,18 +103,23 @@ __global__ void __launch_bounds__(256) batch_init_kernel(BatchArgs a, int nprob,
   if (pid >= nprob) return;
   const BatchProblem pr = a.problems[pid];
   const T* in = static_cast<const T*>(a.arena_a) + pr.offset;
-  const T gamma = (T)a.gamma, gm1 = gamma - T(1);
+  const T gamma = (T)a.gamma, gm1 = gamma - T(1), pinf = (T)a.pinf;
+  const bool stiff = a.pinf != 0.0;
   const int64_t cells = pr.n0 * pr.n1;
   double local = 0.0;
   for (int64_t i = threadIdx.x; i < cells; i += blockDim.x) {
     if (pr.dims == 1) {
       Cons<T, 1> u;
       for (int c = 0; c < 3; ++c) u.v[c] = in[c * pr.pitch + i];
-      ws_max(local, (double)max_wavespeed_q(derive(u, gm1), gamma));
+      const Derived<T, 1> q = derive(u, gm1);
+      ws_max(local, (double)(stiff ? max_wavespeed_q<true>(q, gamma, pinf)
+                                   : max_wavespeed_q<false>(q, gamma)));
     } else {
       Cons<T, 2> u;
       for (int c = 0; c < 4; ++c) u.v[c] = in[c * pr.pitch + i];
-      ws_max(local, (double)max_wavespeed_q(derive(u, gm1), gamma));
+      const Derived<T, 2> q = derive(u, gm1);
+      ws_max(local, (double)(stiff ? max_wavespeed_q<true>(q, gamma, pinf)
+                                   : max_wavespeed_q<false>(q, gamma)));
     }
   }
   const double m = cta_max<8>(local, s_red);
@@ -149,9 +155,11 @@ __global__ void batch_reset_queue_kernel(int* queue) { *queue = 0; }
 template <typename T, int FLUX>
 __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c0, int c1,
                                              T gamma, T gm1, T adi, T dtdh, int limiter,
-                                             bool muscl, bool flatten, double& ws_local) {
+                                             bool muscl, bool flatten, double& ws_local,
+                                             T pinf) {
   constexpr int D = 1;
   constexpr int NC = 3;
+  constexpr bool STIFF = (FLUX & kStiffEos) != 0;
   const T hd = T(0.5) * dtdh;
   const T chi_init = (sizeof(T) == 8) ? (T)DBL_MAX : (T)FLT_MAX;
   Cons<T, D> U[5];
@@ -210,7 +218,7 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
     if (j >= c0) {
       Cons<T, D> fx;
       riemann_q<FLUX>(er_prev, derive(er_prev, gm1), el, derive(el, gm1), 0, gamma, gm1, adi,
-                      dtdh, fx);
+                      dtdh, fx, pinf);
       if (j >= c0 + 1) {
         const Cons<T, D>& uo = U[0];
         Cons<T, D> r;
@@ -218,7 +226,7 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
         for (int c = 0; c < NC; ++c) r.v[c] = uo.v[c] + dtdh * (f_prev.v[c] - fx.v[c]);
 #pragma unroll
         for (int c = 0; c < NC; ++c) dst[c * ld + 4 + (j - 1)] = r.v[c];
-        ws_max(ws_local, (double)max_wavespeed_q(derive(r, gm1), gamma));
+        ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
       }
       f_prev = fx;
     }
@@ -253,6 +261,7 @@ __global__ void __launch_bounds__(THREADS) batch1d_kernel(BatchArgs a, long long
   __shared__ StepControl s_ctrl;
   const T gamma = (T)a.gamma, gm1 = gamma - T(1);
   const T adi = (gamma + T(1)) / (T(2) * gamma);
+  const T pinf = (T)a.pinf;
   const bool muscl = !a.basic;
   const bool flatten = muscl && a.flatten;
   const bool reflect = (a.reflect & 1u) != 0;
@@ -283,7 +292,7 @@ __global__ void __launch_bounds__(THREADS) batch1d_kernel(BatchArgs a, long long
       double ws = 0.0;
       if (c0 < n)
         walk_line_1d<T, FLUX>(cur, nxt, ld, c0, c1, gamma, gm1, adi, dtdh, a.limiter, muscl,
-                              flatten, ws);
+                              flatten, ws, pinf);
       const double m = cta_max<THREADS / 32>(ws, s_red);
       if (threadIdx.x == 0) advance_control(s_ctrl, m, true);
       __syncthreads();
@@ -317,7 +326,7 @@ __global__ void __launch_bounds__(WalkCfg<T, S>::THREADS) batch2d_kernel(BatchAr
   p.n[1] = pr.n1;
   p.n[2] = 1;
   p.gamma = a.gamma;
-  p.pinf = 0.0;                                      // batched problems are ideal gases
+  p.pinf = a.pinf;
   p.dtdh = 0.0;
   p.limiter = a.limiter;
   p.basic = a.basic;

@@ -39,6 +39,7 @@ struct fl_batch {
   int flatten = 1;
   uint32_t reflect = 0;
   double gamma = 1.4;
+  double pinf = 0.0;            // stiffened fluid's p_inf; 0 for the ideal gas
   std::vector<fl_batch_desc> desc;
   // device data
   BatchProblem* d_problems = nullptr;
@@ -158,6 +159,7 @@ BatchArgs base_args(const fl_batch* b) {
   a.arena_a = b->arena_a;
   a.arena_b = b->arena_b;
   a.gamma = b->gamma;
+  a.pinf = b->pinf;
   a.limiter = b->limiter;
   a.basic = b->basic;
   a.flatten = b->flatten;
@@ -180,10 +182,14 @@ cudaError_t prepare(const fl_batch* b) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 64 && done[dev]) return cudaSuccess;
+  constexpr int kSH = kHllc | kStiffEos, kSF = kForce | kStiffEos;
   const cudaError_t r[] = {
       set_attr_1d<T, kHllc, 64>(), set_attr_1d<T, kHllc, 128>(), set_attr_1d<T, kHllc, 256>(),
       set_attr_1d<T, kHllc, 512>(), set_attr_1d<T, kForce, 64>(), set_attr_1d<T, kForce, 128>(),
-      set_attr_1d<T, kForce, 256>(), set_attr_1d<T, kForce, 512>()};
+      set_attr_1d<T, kForce, 256>(), set_attr_1d<T, kForce, 512>(),
+      set_attr_1d<T, kSH, 64>(), set_attr_1d<T, kSH, 128>(), set_attr_1d<T, kSH, 256>(),
+      set_attr_1d<T, kSH, 512>(), set_attr_1d<T, kSF, 64>(), set_attr_1d<T, kSF, 128>(),
+      set_attr_1d<T, kSF, 256>(), set_attr_1d<T, kSF, 512>()};
   for (cudaError_t x : r)
     if (x != cudaSuccess) return x;
   if (dev < 64) done[dev] = true;
@@ -259,13 +265,20 @@ cudaError_t enqueue_steps(fl_batch* b, int64_t nsteps, cudaStream_t st, bool do1
   return cudaSuccess;
 }
 
+template <typename T>
+cudaError_t enqueue_t(fl_batch* b, int64_t nsteps, cudaStream_t st, bool do1d, bool do2d) {
+  switch (b->flux | (b->pinf != 0.0 ? kStiffEos : 0)) {
+    case kForce: return enqueue_steps<T, kForce>(b, nsteps, st, do1d, do2d);
+    case kForce | kStiffEos: return enqueue_steps<T, kForce | kStiffEos>(b, nsteps, st, do1d, do2d);
+    case kHllc | kStiffEos: return enqueue_steps<T, kHllc | kStiffEos>(b, nsteps, st, do1d, do2d);
+    default: return enqueue_steps<T, kHllc>(b, nsteps, st, do1d, do2d);
+  }
+}
+
 cudaError_t enqueue(fl_batch* b, int64_t nsteps, cudaStream_t st, bool do1d = true,
                     bool do2d = true) {
-  if (b->f32)
-    return b->flux == kForce ? enqueue_steps<float, kForce>(b, nsteps, st, do1d, do2d)
-                             : enqueue_steps<float, kHllc>(b, nsteps, st, do1d, do2d);
-  return b->flux == kForce ? enqueue_steps<double, kForce>(b, nsteps, st, do1d, do2d)
-                           : enqueue_steps<double, kHllc>(b, nsteps, st, do1d, do2d);
+  return b->f32 ? enqueue_t<float>(b, nsteps, st, do1d, do2d)
+                : enqueue_t<double>(b, nsteps, st, do1d, do2d);
 }
 
 int64_t arena_elems(const fl_batch* b) {
@@ -351,6 +364,21 @@ int fl_batch_destroy(fl_batch* b) {
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
   delete b;
+  return kOk;
+}
+
+int fl_batch_set_material(fl_batch* b, const fl_material* mat) {
+  if (b == nullptr) return bfail(kEInval, "batch handle is NULL");
+  if (mat == nullptr) return bfail(kEInval, "material is NULL");
+  if (!(mat->gamma > 1.0)) return bfail(kEInval, "gamma must exceed 1");
+  if (!(mat->p_inf >= 0.0) || mat->p_inf > DBL_MAX)
+    return bfail(kEInval, "p_inf must be finite and >= 0");
+  b->gamma = mat->gamma;
+  b->pinf = mat->p_inf;
+  if (b->graph) {  // a captured graph holds the old material's kernels
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
   return kOk;
 }
 

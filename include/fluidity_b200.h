@@ -293,6 +293,10 @@ int fl_batch_create(fl_batch** batch, const fl_batch_desc* problems, int32_t cou
                     double gamma, uint32_t policy, uint32_t boundary_mask);
 int fl_batch_destroy(fl_batch* batch);
 
+/* Gives every problem of the batch the material (gamma and p_inf; p_inf > 0
+ * the stiffened fluid).  Call before fl_batch_begin; drops a captured graph. */
+int fl_batch_set_material(fl_batch* batch, const fl_material* mat);
+
 /* Per-problem initial wavespeed and dt (cfl, stop time, step limit shared). */
 int fl_batch_begin(fl_batch* batch, void* arena_a, void* arena_b, double cfl,
                    double sim_time, int64_t max_iters, void* stream);

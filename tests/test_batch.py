@@ -125,3 +125,56 @@ def test_batch_sim_time_stop(cuda, oracle):
         if np.isfinite(ref).all() and rit < 400:
             assert it[i] == rit
             assert abs(rt[i] - rrt) <= 1e-12 * rrt
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("flux", ["hllc", "force"])
+def test_batch_stiffened_fluid_matches_oracle(cuda, oracle, dtype, flux):
+    """Every problem of the batch as the stiffened fluid (p_inf = 0.613, the
+    bubble of the two-material tests) against the oracle's stiffened loop;
+    the filled states and the step count per problem as well."""
+    import torch
+    from fluidity_b200.batch import Batch
+    p_inf = 0.613
+    probs = small_problems(seed=13, n1d=12, n2d=4)
+    b = Batch(probs, dtype=dtype, flux=flux, p_inf=p_inf)
+    b.fill()
+    steps = 10
+    b.begin(0.8, 1e30, steps)
+    b.capture(steps)
+    b.launch()
+    it, _, _, _ = b.status(allow_nan=True)
+    torch.cuda.synchronize()
+    npdt = np.float64 if dtype == "f64" else np.float32
+    checked = 0
+    with oracle.stiffened(p_inf):
+        for i, (shape, states) in enumerate(probs):
+            u0 = oracle.fill_riemann(shape, states, GAMMA, dtype=npdt)
+            ref, rit, _, _ = oracle.simulate(shape, u0, npdt(GAMMA), npdt(0.8), 1.0 / shape[0],
+                                             npdt(1e30), steps, flux=flux)
+            if not np.isfinite(ref).all():
+                continue
+            assert it[i] == rit == steps, (i, shape)
+            got = b.state(i).double().cpu().numpy()
+            tol = 1e-10 if dtype == "f64" else 2e-4
+            floor = 1e-3 if dtype == "f64" else 1.0
+            assert rel_err(got, ref, floor) < tol, (i, shape)
+            checked += 1
+    assert checked >= len(probs) // 2
+    # the ideal gas on the same data takes other steps
+    g = Batch(probs, dtype=dtype, flux=flux)
+    g.fill()
+    g.begin(0.8, 1e30, steps)
+    g.steps(steps)
+    torch.cuda.synchronize()
+    assert not torch.equal(g.a, b.a)
+
+
+def test_batch_set_material_checks():
+    from fluidity_b200 import build, capi
+    build.build()
+    lib = capi.load()
+    m = capi.Material(GAMMA, 1.0)
+    assert lib.fl_batch_set_material(None, C.byref(m)) == capi.FL_EINVAL
+    assert lib.fl_adj_set_material(None, C.byref(m)) == capi.FL_EINVAL
