@@ -307,14 +307,23 @@ adjoint_sweep_kernel(AdjointParams p) {
     for (int c = 0; c < NC; ++c)
       r[c] = sLam[c * G::E + e] + sDp[c * G::E + e - ES] + sD0[c * G::E + e] +
              sDm[c * G::E + e + ES];
-    // adjoints of ghost positions -1, -2 (evolve cell -1) and n, n+1
-    // (evolve cell n) fold back onto cells 0, 1 and n-1, n-2
+    // adjoints of the ghost positions fold back onto the cells they mirror:
+    //   ghost -1 (= cell 0):       own part of evolve cell -1 and the left
+    //                              neighbour part of evolve cell 0
+    //   ghost -2 (= cell 1):       left neighbour part of evolve cell -1
+    //   ghost n (= cell n-1):      own part of evolve cell n and the right
+    //                              neighbour part of evolve cell n-1
+    //   ghost n+1 (= cell n-2):    right neighbour part of evolve cell n
+    // (evolve cells -2 and n+1 feed only ghost faces, which carry none).
+    // The neighbour parts are non-zero where the limited slope of cell 0 or
+    // n-1 takes the difference across the wall: at a reflective end, the
+    // normal momentum's 2 m when it is the smaller one-sided difference.
     T m[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) m[c] = T(0);
     if (gs == 0) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) m[c] += sD0[c * G::E + e - ES];
+      for (int c = 0; c < NC; ++c) m[c] += sD0[c * G::E + e - ES] + sDm[c * G::E + e];
     }
     if (gs == 1) {
 #pragma unroll
@@ -322,7 +331,7 @@ adjoint_sweep_kernel(AdjointParams p) {
     }
     if (gs == nS - 1) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) m[c] += sD0[c * G::E + e + ES];
+      for (int c = 0; c < NC; ++c) m[c] += sD0[c * G::E + e + ES] + sDp[c * G::E + e];
     }
     if (gs == nS - 2) {
 #pragma unroll
