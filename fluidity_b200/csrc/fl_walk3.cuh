@@ -104,7 +104,19 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
 #pragma unroll
     for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + base + gy * rs + gx);
   }
+  // the third dimension's chi part of evolve row k - 3, loaded one row ahead
+  // like the state
+  T ct_pre = T(0);
+  if (flatten) {
+    bool f = false;
+    ct_pre = __ldg(xc + base + mirror_index(k_first - 3, nr, f) * rs + gx);
+  }
   for (int64_t k = k_first; k <= k_last; ++k) {
+    const T ct = ct_pre;
+    if (flatten && k < k_last) {
+      bool f = false;
+      ct_pre = __ldg(xc + base + mirror_index(k - 2, nr, f) * rs + gx);
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       U[i] = U[i + 1];
@@ -157,8 +169,6 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
         const T dy = P[2] - P[0];
         const int sy = (T(0) < dy) - (dy < T(0));
         const T cr = std_min(CHY[1], sy > 0 ? CHY[2] : (sy < 0 ? CHY[0] : CHY[1]));
-        bool fjy = false;
-        const T ct = __ldg(xc + base + mirror_index(j, nr, fjy) * rs + gx);
         // minimum over dimensions 0, 1, 2 in order
         chi_v = (DR == 1) ? std_min(std_min(std_min(chi_init, cx), cr), ct)
                           : std_min(std_min(std_min(chi_init, cx), ct), cr);
