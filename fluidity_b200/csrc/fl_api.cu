@@ -313,9 +313,34 @@ int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy) {
   return (int64_t)(grid->dims + 2) * grid->pitch * (int64_t)elem_size(decode(policy));
 }
 
+}  // extern "C"
+
+namespace fl {
+int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
+                        const fl_material* mat, double dtdh, uint32_t policy,
+                        uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
+                        int walk_slot, void* stream);
+}  // namespace fl
+
+extern "C" {
+
 int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
                        const fl_material* mat, double dtdh, uint32_t policy,
                        uint32_t boundary_mask, double* max_ws_out, void* stream) {
+  return fl::split_sweep_counted(grid, dim, in, out, mat, dtdh, policy, boundary_mask,
+                                 max_ws_out, nullptr, 0, stream);
+}
+
+}  // extern "C"
+
+namespace fl {
+
+// fl_split_sweep_mat with strip counters (nullable) and their parity slot;
+// the two-material loop owns a pair.
+int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
+                        const fl_material* mat, double dtdh, uint32_t policy,
+                        uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
+                        int walk_slot, void* stream) {
   int rc = check_grid(grid);
   if (rc) return rc;
   if ((rc = check_policy(policy))) return rc;
@@ -329,6 +354,8 @@ int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
   SweepParams p = make_params(grid, pol, mat->gamma, mat->p_inf, dtdh, boundary_mask);
   p.in = in;
   p.out = out;
+  p.walk_next = walk_next;
+  p.walk_slot = walk_slot;
   if (max_ws_out != nullptr) {
     cudaError_t e = cudaMemsetAsync(max_ws_out, 0, sizeof(double), st);
     if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
@@ -350,6 +377,10 @@ int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
   if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
   return kOk;
 }
+
+}  // namespace fl
+
+extern "C" {
 
 int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out, double gamma,
                    double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,

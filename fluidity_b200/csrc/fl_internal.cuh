@@ -58,7 +58,9 @@ struct SweepParams {
   // walk_next[walk_slot] and clearing the other counter for the next sweep
   unsigned int* walk_next;
   int walk_slot;
+  int walk_ry;  // rows per strip of a dynamically scheduled 2-D walk (0: the compiled length)
 };
+
 
 __host__ __device__ __forceinline__ bool ws_row_counts(const SweepParams& p, int64_t row) {
   return p.ws_hi <= p.ws_lo || (row >= p.ws_lo && row < p.ws_hi);

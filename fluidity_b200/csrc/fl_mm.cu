@@ -30,6 +30,14 @@
 #include "fl_internal.cuh"
 
 namespace fl {
+// One dimensional sweep of the split step with strip counters (nullable) and
+// the counters' parity slot: fl_split_sweep_mat for callers that own
+// counters (the two-material loop).
+int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
+                        const fl_material* mat, double dtdh, uint32_t policy,
+                        uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
+                        int walk_slot, void* stream);
+
 namespace {
 
 struct MMCounters {
@@ -446,6 +454,8 @@ using namespace fl;
 
 struct fl_mm {
   fl_grid grid;
+  unsigned int* walk_next = nullptr;  // strip counters of the split sweeps (2, device)
+  int64_t walk_launches = 0;          // sweeps launched with them: the parity slot
   uint32_t policy;
   bool f32;
   double gamma[2];
@@ -480,6 +490,7 @@ namespace {
 void free_mm(fl_mm* m) {
   if (!m) return;
   cudaFree(m->cnt);
+  cudaFree(m->walk_next);
   for (int k = 0; k < 2; ++k) {
     cudaFree(m->band_list[k]);
     cudaFree(m->gfm_idx[k]);
@@ -601,6 +612,8 @@ int fl_mm_create(fl_mm** out, const fl_grid* grid, const double* gammas, uint32_
   const int64_t n = grid->n[0] * grid->n[1];
   const int64_t lsb = fl_ls_workspace_bytes(grid);
   cudaError_t e = cudaMalloc(&m->cnt, sizeof(MMCounters));
+  if (e == cudaSuccess) e = cudaMalloc(&m->walk_next, 2 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(m->walk_next, 0, 2 * sizeof(unsigned int));
   for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
     e = cudaMalloc(&m->band_list[k], n * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&m->gfm_idx[k], n * sizeof(int));
@@ -800,11 +813,16 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     const double dt = m->cfl * m->h / w;
     const double dtdh = dt / m->h;
     // 4: each material's split step with its own gamma; state returns to buffer 0
+    // split_solver.cuh:67-79 per material: sweep x into the second buffer,
+    // y back into the first, with strip counters of their own
     for (int mat = 0; mat < 2; ++mat) {
-      void* in = m->u[mat][0];
-      void* out = m->u[mat][1];
       const fl_material mm{m->gamma[mat], m->pinf[mat]};
-      rc = fl_split_solve_mat(g, &in, &out, &mm, dtdh, m->policy, 0u, nullptr, stream);
+      for (int d = 0; d < 2 && rc == 0; ++d) {
+        void* in = m->u[mat][d];
+        void* out = m->u[mat][1 - d];
+        rc = split_sweep_counted(g, d, in, out, &mm, dtdh, m->policy, 0u, nullptr,
+                                 m->walk_next, (int)(m->walk_launches++ & 1), stream);
+      }
       if (rc) return rc;
     }
     // 5: level sets (multimaterial_simulator.hpp:428-477)

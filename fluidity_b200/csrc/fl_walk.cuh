@@ -287,16 +287,17 @@ walk_kernel_2d(SweepParams p) {
     const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
     walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0, W::RY, ws_local, want_ws);
   } else {
+    const int ry = (p.walk_ry > 0) ? p.walk_ry : W::RY;
     const int64_t ncol = (p.n[0] + W::OWN - 1) / W::OWN;
-    const int64_t items = ncol * ((p.n[1] + W::RY - 1) / W::RY);
+    const int64_t items = ncol * ((p.n[1] + ry - 1) / ry);
     unsigned int* next = &p.walk_next[p.walk_slot];
     for (;;) {
       unsigned int item = 0u;
       if ((threadIdx.x & 31) == 0) item = atomicAdd(next, 1u);
       item = __shfl_sync(0xffffffffu, item, 0);
       if ((int64_t)item >= items) break;
-      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)item % ncol, ((int64_t)item / ncol) * W::RY,
-                                W::RY, ws_local, want_ws);
+      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)item % ncol, ((int64_t)item / ncol) * ry, ry,
+                                ws_local, want_ws);
     }
   }
   if (want_ws) {
