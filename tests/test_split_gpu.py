@@ -480,3 +480,51 @@ def test_f32_l1_against_f64_oracle(cuda, oracle, seed):
     print(f"seed {seed}: FP32 steps {it} (FP64 {steps}), relative L1 per component {l1}")
     assert abs(it - steps) <= 2
     assert np.all(l1 < 1e-4)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(2048, 2048), (1024, 1024), (700, 300)])
+def test_dynamic_strips_equal_static_grid(cuda, dtype, shape):
+    """The device-resident loop takes its strips dynamically (64-row strips
+    at 2048^2, shortened to 32 rows where 64-row strips cannot fill the
+    GPU); fl_split_solve launches the static grid.  Two steps of each, with
+    the loop's own time steps replayed on the static path, agree bit for
+    bit in FP64: the schedule decides only which warp computes a cell.  The
+    two schedules are separately inlined copies of the strip code (one call
+    site for both measured 6-11% slower), and in FP32 the compiler's
+    contractions differ between the copies by a few ulps (6e-7 relative
+    measured), so FP32 agrees to rounding."""
+    import torch
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    s = SplitSolver(shape, dtype=dtype, gamma=GAMMA)
+    a = s.new_state()
+    s.fill_riemann(riemann_states(7, 2), out=a)
+    u0 = a.clone()
+    b = torch.empty_like(a)
+    res = 1.0 / shape[0]
+    sim = Simulation(s)
+    sim.begin(a, b, 0.8, res, 1e30, 2)
+    sim.steps(2)
+    it, _, done, out = sim.status()
+    assert it == 2 and done
+    x, y = u0.clone(), torch.empty_like(u0)
+    ws = s.max_wavespeed(x).item()
+    for _ in range(2):
+        # the time step as the device computes it (finalize_control)
+        if dtype == "f32":
+            f32, f64 = np.float32, np.float64
+            dt = f32(f64(f32(0.8)) * res / f64(f32(ws)))
+            dtdh = float(f32(f64(dt) / res))
+        else:
+            dtdh = (0.8 * res / ws) / res
+        mws = torch.zeros(1, dtype=torch.float64, device="cuda")
+        _, x = s.solve(x, y, dtdh, max_ws=mws)      # 2-D: the result returns to x
+        ws = mws.item()
+    torch.cuda.synchronize()
+    if dtype == "f64":
+        assert torch.equal(out, x)
+    else:
+        d = (out.double() - x.double()).abs()
+        worst = (d / x.double().abs().clamp_min(1.0)).max().item()
+        assert worst < 1e-5, worst
