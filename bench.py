@@ -60,6 +60,10 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-mm", action="store_true")
+    p.add_argument("--no-e2e", action="store_true",
+                   help="skip the end-to-end host-buffer leg (profiling captures)")
+    p.add_argument("--no-correctness", action="store_true",
+                   help="skip the L1-vs-FP64 and conservation figures")
     p.add_argument("--mm-steps", type=int, default=500)
     p.add_argument("--only", choices=["mm", "adjoint", "batched", "3d"], default=None,
                    help="run one secondary workload alone (profiling); prints its own line")
@@ -326,34 +330,45 @@ def run_ours(a, world, rank, local):
     # download overlap job k's compute.  Every step's copies are inside the
     # timed region; the first upload and the last download are not hidden.
     from fluidity_b200.solver import HostPipeline
-    pinned_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
-    s.fill_riemann(states, out=buf_a)
-    pinned_in.copy_(buf_a)
-    torch.cuda.synchronize()
-    e2e_steps = max(2, min(a.steps, 5))
-    pinned_out = [torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
-                  for _ in range(e2e_steps)]
-    pipe = HostPipeline(s, sets=3)
-    pipe.run([pinned_in], pinned_out[:1], 0.8, 1.0 / a.size, 1e30, T)     # warm-up
-    barrier(world)
-    t0 = time.perf_counter()
-    jobs = pipe.run([pinned_in] * e2e_steps, pinned_out, 0.8, 1.0 / a.size, 1e30, T)
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, world, dev)
-    if any(it2 != T for it2, _ in jobs):
-        raise RuntimeError("end-to-end run did not complete")
-    e2e_value = world * cells * T * e2e_steps / e2e_s
     state_bytes = nc * elem * cells
-    del pipe
+    e2e_steps, e2e_value = 0, None
+    if not a.no_e2e:
+        pinned_in = torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
+        s.fill_riemann(states, out=buf_a)
+        pinned_in.copy_(buf_a)
+        torch.cuda.synchronize()
+        e2e_steps = max(2, min(a.steps, 5))
+        pinned_out = [torch.empty(buf_a.shape, dtype=buf_a.dtype, pin_memory=True)
+                      for _ in range(e2e_steps)]
+        pipe = HostPipeline(s, sets=3)
+        pipe.run([pinned_in], pinned_out[:1], 0.8, 1.0 / a.size, 1e30, T)     # warm-up
+        barrier(world)
+        t0 = time.perf_counter()
+        jobs = pipe.run([pinned_in] * e2e_steps, pinned_out, 0.8, 1.0 / a.size, 1e30, T)
+        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, world, dev)
+        if any(it2 != T for it2, _ in jobs):
+            raise RuntimeError("end-to-end run did not complete")
+        e2e_value = world * cells * T * e2e_steps / e2e_s
+        del pipe
 
     variants = {}
+    ref_cache = {}
+    headline_checks = None
+    if rank == 0 and world == 1 and not a.no_correctness:
+        headline_checks = correctness(2, a.size, a.dtype, a.flux, ref_cache)
     if not a.no_variants and rank == 0:
-        for dt_, fx in (("f32", "hllc"), ("f64", "force"), ("f32", "force")):
+        for dt_, fx in (("f64", "hllc"), ("f32", "hllc"), ("f64", "force"), ("f32", "force")):
             if (dt_, fx) == (a.dtype, a.flux):
                 continue
             variants[f"{fx}_{dt_}"] = measure_variant(a, dt_, fx, states)
-        for dt_ in ("f64", "f32"):
-            variants[f"3d_hllc_{dt_}"] = measure_3d(dt_)
+            if not a.no_correctness:
+                variants[f"{fx}_{dt_}"].update(correctness(2, a.size, dt_, fx, ref_cache))
+        for fx in ("hllc", "force"):
+            for dt_ in ("f64", "f32"):
+                variants[f"3d_{fx}_{dt_}"] = measure_3d(dt_, flux=fx)
+                if not a.no_correctness:
+                    variants[f"3d_{fx}_{dt_}"].update(correctness(3, 256, dt_, fx, ref_cache))
 
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
@@ -377,6 +392,8 @@ def run_ours(a, world, rank, local):
         "gpu_launches": a.steps * (3 + launches_per_run),
         "clocks": clocks,
     }
+    if headline_checks is not None:
+        line.update(headline_checks)
     if variants:
         line["variants"] = variants
     if rank == 0 and world == 1 and not a.no_batched:
@@ -458,6 +475,79 @@ def measure_3d(dtype, flux="hllc", n=256, steps=20, runs=3):
     return {"workload": f"3-D octant Riemann problem {n}^3, {steps} steps, {flux.upper()}",
             "cell_updates_per_s": cells * steps * runs / (total / 1e3), "sweep_gbs": gbs,
             "frac_of_measured_hbm": gbs / peak, "steps_completed": it}
+
+
+PARITY_BARS = {
+    "f64": "1e-12 relative per cell and sweep against the reference's functors "
+           "(relative to max(|ref|, 1e-3 of the component's largest magnitude))",
+    "f32": "1e-5 of the component's largest magnitude per cell and sweep against the FP32 "
+           "restatement of the reference's arithmetic",
+}
+
+
+def correctness(dims, n, dtype, flux, ref_cache, steps=2):
+    """Per-result correctness figures of one workload variant.
+
+    l1_vs_fp64: relative L1 per component (sum |x - ref| / sum |ref|) of the
+    state after `steps` time steps of the run (device-resident loop, same
+    kernels as the timed run) against the FP64 reference run of the same
+    steps from the same initial data: the reference's own functors
+    (oracle/_ref) on the host cores, or the pinned C oracle where that
+    library is absent.
+
+    conservation: for each sweep of those steps, the residual of
+    sum U_out - sum U_in - dtdh (inflow - outflow) per component, relative to
+    sum |U_in| + the boundary flux magnitudes (fluidity_b200/diagnostics.py):
+    mass, momentum and energy change only by the flux through the
+    transmissive ends, to round-off."""
+    import torch
+    from oracle import oracle
+    from fluidity_b200.diagnostics import l1_relative, sweep_conservation_residual
+    from fluidity_b200.solver import Simulation, SplitSolver
+    from fluidity_b200.workloads import riemann_states
+    shape = (n,) * dims
+    st = riemann_states(SEED, dims)
+    key = (dims, n, flux, steps)
+    if key not in ref_cache:
+        u0 = oracle.fill_riemann(shape, st, GAMMA)
+        t0 = time.perf_counter()
+        if oracle.ref_available():
+            ref, k, _, _ = oracle.ref_simulate(shape, u0, GAMMA, 0.8, 1.0 / n, 1e30, steps,
+                                               flux=flux)
+            kind = "reference functors (oracle/_ref)"
+        else:
+            ref, k, _, _ = oracle.simulate(shape, u0, GAMMA, 0.8, 1.0 / n, 1e30, steps, flux=flux)
+            kind = "C oracle (pinned to the reference's functors)"
+        ref_cache[key] = (torch.from_numpy(ref), k, kind, time.perf_counter() - t0)
+        del u0
+    ref, k, kind, ref_s = ref_cache[key]
+    s = SplitSolver(shape, dtype=dtype, flux=flux, gamma=GAMMA)
+    a = s.fill_riemann(st)
+    b = torch.empty_like(a)
+    res, it, _ = Simulation(s).run(a, b, 0.8, 1.0 / n, 1e30, steps)
+    l1 = l1_relative(res.cpu(), ref, shape)
+    # conservation of each sweep of the same steps
+    a = s.fill_riemann(st)
+    worst = {}
+    for _ in range(steps):
+        dtdh = 0.8 / s.max_wavespeed(a).item()
+        for dim in range(dims):
+            s.sweep(a, b, dim, dtdh)
+            for c, v in sweep_conservation_residual(shape, a, b, dim, dtdh, GAMMA).items():
+                worst[c] = max(worst.get(c, 0.0), v)
+            a, b = b, a
+    torch.cuda.synchronize()
+    del a, b, res, s
+    torch.cuda.empty_cache()
+    return {
+        "l1_vs_fp64": {"steps": int(it), "reference": kind, "reference_steps": int(k),
+                       "per_component": {c: float(f"{v:.3g}") for c, v in l1.items()}},
+        "conservation": {"sweeps": steps * dims, "max_rel_residual":
+                         {c: float(f"{v:.3g}") for c, v in worst.items()},
+                         "check": "sum U_out - sum U_in - dtdh * (flux through the "
+                                  "transmissive ends) per sweep, over sum |U_in|"},
+        "parity_bar": PARITY_BARS[dtype],
+    }
 
 
 def measure_batched(seed=3, steps=200, baseline_every=4):

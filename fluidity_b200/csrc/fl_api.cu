@@ -298,9 +298,26 @@ struct fl_sim {
   unsigned long long* ws_word;  // external: the caller's device word (else ctrl->ws_bits)
   int cursor;              // next sweep of the current step (fl_sim_sweep)
   void* scratch;           // 3-D: the walk's chi plane (else nullptr)
+  // a counted sweep failed to launch: it neither took its strips nor
+  // cleared the other counter, so both are re-zeroed before the next sweep
+  int counters_dirty;
 };
 
 using namespace fl;
+
+namespace {
+
+// Re-zeroes both strip counters of sim's control block on the stream when a
+// counted sweep failed before (the failed launch cleared neither).
+int settle_counters(fl_sim* sim, cudaStream_t st, const char* where) {
+  if (!sim->counters_dirty) return kOk;
+  cudaError_t e = cudaMemsetAsync(sim->ctrl->walk_next, 0, sizeof(sim->ctrl->walk_next), st);
+  if (e != cudaSuccess) return cuda_fail(e, where);
+  sim->counters_dirty = 0;
+  return kOk;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -551,6 +568,7 @@ int fl_sim_begin(fl_sim* sim, void* a, void* b, double cfl, double res, double s
                                         sim->pol.f32 ? 1 : 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "fl_sim_begin");
+  sim->counters_dirty = 0;  // the control block's initialisation zeroes both counters
   sim->cursor = 0;
   if (sim->external && sim->ws_word == nullptr)
     return fail(kEInval, "external reduction needs fl_sim_set_ws_word");
@@ -582,6 +600,8 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
   if (sim->external) return fail(kEInval, "external reduction: step with fl_sim_sweep");
   if (sim->cursor != 0) return fail(kEInval, "a step is half done (fl_sim_sweep)");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = settle_counters(sim, st, "fl_sim_steps");
+  if (rc) return rc;
   const int D = sim->grid.dims;
   SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, sim->pinf, 0.0, sim->boundary);
   p.ctrl = sim->ctrl;
@@ -603,7 +623,10 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
       p.ws_accum = last ? &sim->ctrl->ws_bits : nullptr;
       p.finalize = last ? 1 : 0;
       cudaError_t e = launch_sweep(p, sim->pol, D, d, st);
-      if (e != cudaSuccess) return cuda_fail(e, "fl_sim_steps");
+      if (e != cudaSuccess) {
+        sim->counters_dirty = 1;
+        return cuda_fail(e, "fl_sim_steps");
+      }
       if (D != 1 && d < D - 1) {
         void* t = si;
         si = so;
@@ -653,6 +676,8 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   if (sim == nullptr || sim->a == nullptr) return fail(kEInval, "fl_sim_begin not called");
   const int D = sim->grid.dims;
   if (dim != sim->cursor) return fail(kEInval, "sweep %d expected, %d given", sim->cursor, dim);
+  int rc = settle_counters(sim, static_cast<cudaStream_t>(stream), "fl_sim_sweep");
+  if (rc) return rc;
   const bool from_b = (D % 2 == 1) && ((sim->enqueued & 1) == 1);
   void* si = from_b ? sim->b : sim->a;
   void* so = from_b ? sim->a : sim->b;
@@ -674,7 +699,10 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   p.ws_accum = last ? (sim->external ? sim->ws_word : &sim->ctrl->ws_bits) : nullptr;
   p.finalize = (last && !sim->external) ? 1 : 0;
   cudaError_t e = launch_sweep(p, sim->pol, D, dim, static_cast<cudaStream_t>(stream));
-  if (e != cudaSuccess) return cuda_fail(e, "fl_sim_sweep");
+  if (e != cudaSuccess) {
+    sim->counters_dirty = 1;
+    return cuda_fail(e, "fl_sim_sweep");
+  }
   if (last) {
     sim->cursor = 0;
     sim->enqueued += 1;
@@ -749,15 +777,6 @@ static __device__ __align__(256) fl::StepControl g_noalloc_control[1];
 
 }  // extern "C"
 
-namespace {
-
-// Device address of g_noalloc_control, resolved once per device with that
-// device current.  (The host-side name of the array is a stand-in, not a
-// device address, and must never be handed to a kernel.)
-fl::StepControl* g_noalloc_addr[64] = {nullptr};
-
-}  // namespace
-
 extern "C" {
 
 int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
@@ -774,14 +793,15 @@ int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "fl_simulate_noalloc");
-  if (dev < 0 || dev >= 64) return fail(kEInval, "device ordinal %d beyond the 64 supported", dev);
-  if (g_noalloc_addr[dev] == nullptr) {
-    // first call on this device: the set-up, outside any stream capture
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_control);
-    if (e != cudaSuccess) return cuda_fail(e, "fl_simulate_noalloc: cudaGetSymbolAddress");
-    g_noalloc_addr[dev] = static_cast<fl::StepControl*>(p);
-  }
+  // The device address of the array, resolved on every call with the
+  // caller's device current: the host-side name of the array is a stand-in,
+  // not a device address, and a cached address would go stale when the
+  // context is rebuilt (cudaDeviceReset reloads the module).  Resolving it is
+  // a lookup, not an allocation; the first call on a device may load the
+  // library's module there, so it should come before any stream capture.
+  void* ctrl_addr = nullptr;
+  e = cudaGetSymbolAddress(&ctrl_addr, g_noalloc_control);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_simulate_noalloc: cudaGetSymbolAddress");
   fl_sim sim;
   memset(&sim, 0, sizeof(sim));
   sim.grid = *grid;
@@ -790,7 +810,7 @@ int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
   sim.gamma = gamma;
   sim.boundary = boundary_mask;
   sim.device = dev;
-  sim.ctrl = g_noalloc_addr[dev];
+  sim.ctrl = static_cast<fl::StepControl*>(ctrl_addr);
   return fl_simulate(&sim, a, b, cfl, res, sim_time, max_iters, stream, iters, run_time, result);
 }
 

@@ -256,11 +256,15 @@ int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res,
  * deployments that fix their memory up front).  Instead of the control block
  * of fl_sim_create, the loop uses a fixed 96-byte block in a static device
  * array of the library: one per GPU that loads it, held until the process
- * exits; no grid size needs more.  Same arguments and result as
- * fl_sim_create + fl_simulate.  The first call on a device resolves the
- * array's device address, so make it before any stream capture.  Calls on
- * the same GPU share the block: calls that overlap there (two streams or
- * threads) race. */
+ * exits; no grid size needs more.  Same arguments as fl_sim_create +
+ * fl_simulate.  1-D and 2-D results are the same as fl_simulate's bit for
+ * bit; 3-D sweeps take the shared-memory tile kernel (the register walk
+ * needs a scratch plane this entry point cannot allocate), which matches
+ * fl_simulate to rounding, not bit for bit.  Every call resolves the
+ * array's device address with the caller's device current; the first call
+ * on a device may load the library's module there, so make it before any
+ * stream capture.  Calls on the same GPU share the block: calls that
+ * overlap there (two streams or threads) race. */
 int fl_simulate_noalloc(const fl_grid* grid, double gamma, uint32_t policy,
                         uint32_t boundary_mask, void* a, void* b, double cfl, double res,
                         double sim_time, int64_t max_iters, void* stream, int64_t* iters,

@@ -2,8 +2,9 @@
 # Builds oracle/_ref/libfluidity_ref.so: the reference's own numerics functors
 # (robclu/fluidity, header-only) driven by oracle/ref_driver.cpp.
 #
-# TEST INFRASTRUCTURE ONLY.  The reference headers are read from
-# $FLUIDITY_REF (default /root/reference) and copied to a temporary directory
+# TEST INFRASTRUCTURE ONLY.  Usage: build_ref.sh REFERENCE_ROOT (or set
+# FLUIDITY_REF).  The reference headers are read from REFERENCE_ROOT/include
+# and copied to a temporary directory
 # outside the repository, where two one-line fixes are applied without which
 # the host build does not compile (the reference as shipped does not build):
 #   1. flux_method/flux_hllc.hpp: Hllc::get sits in the private section while
@@ -14,7 +15,12 @@
 # Nothing else is changed; no reference source is written into the repository.
 set -euo pipefail
 here="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-src="${FLUIDITY_REF:-/root/reference}/include"
+root="${1:-${FLUIDITY_REF:-}}"
+if [ -z "$root" ]; then
+  echo "build_ref.sh: give the reference checkout as the argument or in FLUIDITY_REF" >&2
+  exit 2
+fi
+src="$root/include"
 if [ ! -d "$src/fluidity" ]; then
   echo "build_ref.sh: reference headers not found at $src" >&2
   exit 2

@@ -39,13 +39,14 @@ class _Policy(C.Structure):
                 ("flatten", C.c_int32), ("reflect", C.c_uint32)]
 
 
-def build() -> None:
-    """Compile liboracle.so (and, when the reference tree is present, the
-    reference-functor library) with the recipes in this folder."""
+def build(ref_root: str | None = None) -> None:
+    """Compile liboracle.so and, when a reference checkout is given (argument
+    or FLUIDITY_REF) and present, the reference-functor library, with the
+    recipes in this folder."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref_root = os.environ.get("FLUIDITY_REF", "/root/reference")
-    if os.path.isdir(os.path.join(ref_root, "include", "fluidity")):
-        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], check=True,
+    ref_root = ref_root or os.environ.get("FLUIDITY_REF")
+    if ref_root and os.path.isdir(os.path.join(ref_root, "include", "fluidity")):
+        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), ref_root], check=True,
                        stdout=subprocess.DEVNULL)
 
 
