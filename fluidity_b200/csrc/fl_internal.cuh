@@ -59,7 +59,18 @@ struct SweepParams {
   unsigned int* walk_next;
   int walk_slot;
   int walk_ry;  // rows per strip of a dynamically scheduled 2-D walk (0: the compiled length)
+  // nullable: a kernel whose bounded wait on its own copies gave up writes
+  // kETimeout here (and stops the loop through ctrl->done when ctrl is set)
+  int* status;
 };
+
+// Tensor map of one SoA state buffer for the TMA-staged sweeps: a 3-D
+// tensor (x, y, component plane) of n0 x n1 x planes elements with rows n0
+// and planes `pitch` elements apart, boxes of box0 x box1 x planes.
+// Returns 0, or an error status with the message recorded.  Defined in
+// fl_tmap.cu; maps are cached per (address, shape, box).
+int encode_state_map(void* map, const void* base, int64_t n0, int64_t n1, int64_t pitch,
+                     int planes, int elem, int box0, int box1);
 
 
 __host__ __device__ __forceinline__ bool ws_row_counts(const SweepParams& p, int64_t row) {
