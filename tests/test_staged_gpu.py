@@ -69,7 +69,10 @@ def _sweeps(shape, dtype, u, dtdh, pol, reflect=0, p_inf=0.0):
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
 @pytest.mark.parametrize("pol", POLICIES, ids=lambda p: "-".join(str(x) for x in p))
 def test_staged_policy_sweeps(cuda, oracle, shape, dtype, pol):
-    u = oracle.prim_to_cons(random_prim(shape, 3, smooth=True), GAMMA, dtype=NPDT[dtype])
+    # moderate contrasts: the full value ranges on grids a few cells wide
+    # drive the oracle itself to negative pressures
+    u = oracle.prim_to_cons(random_prim(shape, 3, smooth=True, mild=True), GAMMA,
+                            dtype=NPDT[dtype])
     ws = float(oracle.max_wavespeed(shape, u, NPDT[dtype](GAMMA)))
     assert _sweeps(shape, dtype, u, 0.4 / ws, pol) < TOL[dtype]
 
@@ -82,6 +85,27 @@ def test_staged_reflective(cuda, oracle, shape, dtype, reflect):
                             dtype=NPDT[dtype])
     ws = float(oracle.max_wavespeed(shape, u, NPDT[dtype](GAMMA)))
     assert _sweeps(shape, dtype, u, 0.4 / ws, POLICIES[0], reflect=reflect) < TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_staged_flattening_active(cuda, oracle, dtype):
+    """An oblique compressive ramp: chi < 1 in both dimensions, across warp
+    boundaries in both sweeps."""
+    shape = (64, 48)
+    prim = np.zeros((4, 64 * 48))
+    x = np.tile(np.arange(64), 48)
+    y = np.repeat(np.arange(48), 64)
+    w = np.clip((x + y - 50) / 4.0, 0.0, 1.0)
+    prim[0] = 3.0 + (0.5 - 3.0) * w
+    prim[1] = 20.0 + (1.0 - 20.0) * w
+    prim[2] = 1.0 + (-0.5 - 1.0) * w
+    prim[3] = 1.0 + (-0.5 - 1.0) * w
+    u = oracle.prim_to_cons(prim, GAMMA, dtype=NPDT[dtype])
+    ws = float(oracle.max_wavespeed(shape, u, NPDT[dtype](GAMMA)))
+    noflat = oracle.sweep(shape, 0, u, NPDT[dtype](GAMMA), NPDT[dtype](0.8 / ws), flatten=False)
+    flat = oracle.sweep(shape, 0, u, NPDT[dtype](GAMMA), NPDT[dtype](0.8 / ws))
+    assert not np.array_equal(flat, noflat), "flattening never triggered"
+    assert _sweeps(shape, dtype, u, 0.8 / ws, POLICIES[0]) < TOL[dtype]
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
