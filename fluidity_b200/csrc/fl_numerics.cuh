@@ -425,12 +425,13 @@ FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
   for (int c = 0; c < D + 2; ++c) f.v[c] = f.v[c] + s * (st.v[c] - u.v[c]);
 }
 
-// FLUX as for riemann.
+// FLUX as for riemann.  dhdt = 1 / dtdh, the Lax-Friedrichs coefficient
+// (flux_lax_friedrichs.hpp:63-78), given by a caller that computes it once.
 template <int FLUX, typename T, int D>
-FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
-                                          const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
-                                          T gamma, T gm1, T adi, T dtdh, Cons<T, D>& f,
-                                          T pinf = T(0)) {
+FL_HD void riemann_qh(const Cons<T, D>& ul, const Derived<T, D>& ql,
+                                           const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
+                                           T gamma, T gm1, T adi, T dtdh, T dhdt, Cons<T, D>& f,
+                                           T pinf = T(0)) {
   constexpr int RS = FLUX & 3;
   if constexpr (RS == kHllc) {
     hllc_q<(FLUX & kStiffEos) != 0>(ul, ql, ur, qr, d, gamma, adi, f, pinf);
@@ -439,7 +440,11 @@ FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
     flux_q(ul, ql, d, fl);
     flux_q(ur, qr, d, fr);
     Cons<T, D> lf, ri;
-    if constexpr (RS != kRichtmyer) lax_friedrichs_ff(ul, ur, fl, fr, dtdh, lf);
+    if constexpr (RS != kRichtmyer) {
+#pragma unroll
+      for (int c = 0; c < D + 2; ++c)
+        lf.v[c] = T(0.5) * (fl.v[c] + fr.v[c] + dhdt * (ul.v[c] - ur.v[c]));
+    }
     if constexpr (RS != kLaxFriedrichs) {
       Cons<T, D> m;
 #pragma unroll
@@ -456,6 +461,14 @@ FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
       for (int c = 0; c < D + 2; ++c) f.v[c] = T(0.5) * (lf.v[c] + ri.v[c]);
     }
   }
+}
+
+template <int FLUX, typename T, int D>
+FL_HD void riemann_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
+                                          const Cons<T, D>& ur, const Derived<T, D>& qr, int d,
+                                          T gamma, T gm1, T adi, T dtdh, Cons<T, D>& f,
+                                          T pinf = T(0)) {
+  riemann_qh<FLUX>(ul, ql, ur, qr, d, gamma, gm1, adi, dtdh, T(1.0) / dtdh, f, pinf);
 }
 
 // The reference's van Leer slope 0.5 (bd + fd) * 2 min(r, 1) / (1 + r) with

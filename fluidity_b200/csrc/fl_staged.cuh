@@ -100,36 +100,36 @@ struct StagedSmem {
 // Box coordinate along the sweep of stage t's first position p0, and whether
 // the stage is a mirror image (its positions map to columns in reverse).
 template <typename T, int S>
-__device__ __forceinline__ int stage_along(int64_t p0, int64_t nl, bool& reversed) {
+__device__ __forceinline__ int stage_along(int p0, int nl, bool& reversed) {
   using C = StagedCfg<T, S>;
   reversed = false;
   if (S == 1) {  // one row per stage: the mirrored row itself
     bool f;
-    return (int)mirror_index(p0, nl, f);
+    return (int)mirror_index((int64_t)p0, (int64_t)nl, f);
   }
   if (p0 < 0) {
     reversed = true;
-    return (int)(-p0 - C::CB);
+    return -p0 - C::CB;
   }
   if (p0 >= nl) {
     reversed = true;
-    return (int)(2 * nl - p0 - C::CB);
+    return 2 * nl - p0 - C::CB;
   }
-  return (int)p0;
+  return p0;
 }
 
 template <typename T, int S>
 __device__ __forceinline__ void stage_issue(const StagedSmem<T, S>& sm, const CUtensorMap* tin,
-                                            int slot, int64_t p0, int64_t nl, int64_t a0) {
+                                            int slot, int p0, int nl, int a0) {
   using C = StagedCfg<T, S>;
   bool rev;
   const int al = stage_along<T, S>(p0, nl, rev);
   T* dst = sm.ring + (size_t)slot * C::STAGE;
   mbar_expect_tx(&sm.bars[slot], C::STAGE_BYTES);
   if (S == 1)
-    tma_load_3d(dst, tin, &sm.bars[slot], (int)(a0 - C::AOFF), al, 0);
+    tma_load_3d(dst, tin, &sm.bars[slot], a0 - C::AOFF, al, 0);
   else
-    tma_load_3d(dst, tin, &sm.bars[slot], al, (int)(a0 - C::AOFF), 0);
+    tma_load_3d(dst, tin, &sm.bars[slot], al, a0 - C::AOFF, 0);
 }
 
 // Component c of the cell at box index `a` of the stage in `slot`, walk
@@ -145,12 +145,13 @@ __device__ __forceinline__ T stage_at(const StagedSmem<T, S>& sm, int slot, int 
 // One warp's strip: across block `ab` (cells a0 = 32 ab .. a0 + 31 across
 // the sweep), positions [s0, s0 + ry) along it.  Stores the updated cells and
 // folds the wavespeed of each stored cell into ws_local.  gstage counts the
-// stages this warp has issued before (ring slot and barrier phase).
+// stages this warp has issued before (ring slot and barrier phase).  Grid
+// extents are below 2^30 (checked by the launcher), so positions are ints.
 template <typename T, int S, int FLUX>
 __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtensorMap* tin,
                                              const CUtensorMap* tout,
-                                             const StagedSmem<T, S>& sm, T dtdh, int64_t ab,
-                                             int64_t s0, int ry, double& ws_local, bool want_ws,
+                                             const StagedSmem<T, S>& sm, T dtdh, T dhdt, int ab,
+                                             int s0, int ry, double& ws_local, bool want_ws,
                                              uint32_t& gstage, int& fault) {
   using Cf = StagedCfg<T, S>;
   constexpr int D = 2;
@@ -168,35 +169,35 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   const T chi_init = (sizeof(T) == 8) ? (T)DBL_MAX : (T)FLT_MAX;
   const int lane = threadIdx.x & 31;
 
-  const int64_t nl = p.n[S];        // cells along the sweep
-  const int64_t na = p.n[1 - S];    // cells across it
-  const int64_t pitch = p.pitch;
-  const int64_t a0 = ab * 32;
+  const int nl = (int)p.n[S];      // cells along the sweep
+  const int na = (int)p.n[1 - S];  // cells across it
+  const int a0 = ab * 32;
   const bool flip_l_on = (p.reflect & (1u << S)) != 0;
   const bool flip_a_on = (p.reflect & (1u << (1 - S))) != 0;
 
   // this lane's cell across the sweep, and the box index it reads
-  const int64_t ai = a0 + lane;
+  const int ai = a0 + lane;
   bool fa = false;
-  const int64_t gai = mirror_index(ai, na, fa);
-  int aoff = (int)(gai - (a0 - Cf::AOFF));
+  const int gai = (int)mirror_index(ai, na, fa);
+  int aoff = gai - (a0 - Cf::AOFF);
   aoff = aoff < 0 ? 0 : (aoff >= Cf::BW ? Cf::BW - 1 : aoff);
   const bool flip_a = fa && flip_a_on;
   const bool owned = ai < na;
   const int own = Cf::AOFF + lane;  // exchange index of this lane's cell
   // lanes 0-5: one across-halo cell each (3 on each side of the warp)
-  const int64_t hai = (lane < 3) ? a0 - 3 + lane : a0 + 29 + lane;
+  const int hai = (lane < 3) ? a0 - 3 + lane : a0 + 29 + lane;
   bool fh = false;
-  const int64_t ghai = mirror_index(hai, na, fh);
-  int hoff = (int)(ghai - (a0 - Cf::AOFF));
+  const int ghai = (int)mirror_index(hai, na, fh);
+  int hoff = ghai - (a0 - Cf::AOFF);
   hoff = hoff < 0 ? 0 : (hoff >= Cf::BW ? Cf::BW - 1 : hoff);
   const bool flip_h = fh && flip_a_on;
   const int hx = (lane < 3) ? Cf::AOFF - 3 + lane : Cf::AOFF + 29 + lane;
 
-  const int64_t s_end = (s0 + ry < nl) ? s0 + ry : nl;
-  const int64_t k_first = s0 - 4;
-  const int64_t k_last = s_end + 3;
-  const int nst = (int)((k_last - k_first + 1 + PPS - 1) / PPS);  // stages of this strip
+  const int s_end = (s0 + ry < nl) ? s0 + ry : nl;
+  const int k_first = s0 - 4;
+  const int k_last = s_end + 3;
+  const int nr = k_last - k_first + 1;
+  const int nst = (nr + PPS - 1) / PPS;  // stages of this strip
   const uint32_t g0 = gstage;
 
   // fill the ring
@@ -206,27 +207,32 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   if (lane == 0) {
     fence_proxy_async_smem();
     for (int t = 0; t < issued; ++t)
-      stage_issue<T, S>(sm, tin, (int)((g0 + t) % NS), k_first + (int64_t)t * PPS, nl, a0);
+      stage_issue<T, S>(sm, tin, (int)((g0 + t) % NS), k_first + t * PPS, nl, a0);
   }
 
-  // reads component planes of the cell at walk offset r (position
-  // k_first + r) for box index a, applying the ghost flips
-  auto cell = [&](int r, int a, bool flip_across) {
+  // the stage holding walk offset r, and r's column within it
+  auto stage_of = [&](int r, int& q) -> const T* {
     const int t = r / PPS;
-    const int slot = (int)((g0 + t) % NS);
-    const int64_t k = k_first + r;
-    int q = r - t * PPS;
-    bool rev = false;
-    if (S == 0) (void)stage_along<T, S>(k_first + (int64_t)t * PPS, nl, rev);
-    if (rev) q = PPS - 1 - q;
+    q = r - t * PPS;
+    if (S == 0) {
+      bool rev;
+      (void)stage_along<T, S>(k_first + t * PPS, nl, rev);
+      if (rev) q = PPS - 1 - q;
+    }
+    return sm.ring + (size_t)((g0 + t) % NS) * Cf::STAGE;
+  };
+  // the cell at box index a of a stage, with the ghost flips: gl along the
+  // sweep (a mirrored position), fx across it (a mirrored lane)
+  auto load = [&](const T* st, int q, int a, bool gl, bool fx) {
     Cons<T, D> u;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) u.v[c] = stage_at<T, S>(sm, slot, q, a, c);
-    const bool gl = (k < 0 || k >= nl) && flip_l_on;
+    for (int c = 0; c < NC; ++c)
+      u.v[c] = (S == 1) ? st[c * Cf::BW + a] : st[(c * Cf::BW + a) * Cf::CB + q];
     if (gl) u.v[2 + S] = (-(u.v[2 + S] / u.v[0])) * u.v[0];
-    if (flip_across) u.v[3 - S] = (-(u.v[3 - S] / u.v[0])) * u.v[0];
+    if (fx) u.v[3 - S] = (-(u.v[3 - S] / u.v[0])) * u.v[0];
     return u;
   };
+  auto ghost_l = [&](int k) { return flip_l_on && (unsigned)k >= (unsigned)nl; };
 
   // windows along the sweep: index 4 = newest position k, k - i at 4 - i
   T P[5], VL[5];
@@ -240,9 +246,11 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
 #pragma unroll
   for (int i = 0; i < 4; ++i) CX[i] = T(1);
 
-  const int nr = (int)(k_last - k_first + 1);
+  T* const out = static_cast<T*>(p.out);
+  const int64_t pitch = p.pitch;
+
   for (int r = 0; r < nr; ++r) {
-    const int64_t k = k_first + r;
+    const int k = k_first + r;
     // ---- ring: recycle the stage the walk no longer reads, wait for k ----
     if (r >= 5 && (r - 5) % PPS == PPS - 1) {
       const int td = (r - 5) / PPS;
@@ -250,8 +258,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
         __syncwarp();
         if (lane == 0) {
           fence_proxy_async_smem();
-          stage_issue<T, S>(sm, tin, (int)((g0 + td) % NS),
-                            k_first + (int64_t)(td + NS) * PPS, nl, a0);
+          stage_issue<T, S>(sm, tin, (int)((g0 + td) % NS), k_first + (td + NS) * PPS, nl, a0);
         }
         ++issued;
       }
@@ -265,7 +272,10 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       }
     }
     // ---- derive position k: own cell, then the across halo ---------------
-    const Cons<T, D> u = cell(r, aoff, flip_a);
+    int qk;
+    const T* stk = stage_of(r, qk);
+    const bool glk = ghost_l(k);
+    const Cons<T, D> u = load(stk, qk, aoff, glk, flip_a);
     const Derived<T, D> q = derive(u, gm1);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -279,7 +289,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       sm.xp[own] = q.p;
       sm.xv[own] = q.v[1 - S];
       if (lane < 6) {
-        const Cons<T, D> uh = cell(r, hoff, flip_h);
+        const Cons<T, D> uh = load(stk, qk, hoff, glk, flip_h);
         const Derived<T, D> qh = derive(uh, gm1);
         sm.xp[hx] = qh.p;
         sm.xv[hx] = qh.v[1 - S];
@@ -307,17 +317,22 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     CHA[1] = CHA[2];
     if (flatten) CHA[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VL[1], VL[3]);
 
-    const int64_t j = k - 3;  // evolve position
+    const int j = k - 3;  // evolve position
     if (j < s0 - 1) continue;
     // ---- evolved face states of (lane, j) ----------------------------------
-    const Cons<T, D> uj = cell(r - 3, aoff, flip_a);
-    const Cons<T, D> um = cell(r - 4, aoff, flip_a);  // position j - 1
+    int qj, qm;
+    const T* stj = stage_of(r - 3, qj);
+    const T* stm = stage_of(r - 4, qm);
+    const Cons<T, D> uj = load(stj, qj, aoff, ghost_l(j), flip_a);
+    const Cons<T, D> um = load(stm, qm, aoff, ghost_l(j - 1), flip_a);  // position j - 1
     Cons<T, D> er, el;
     if (!muscl) {
       er = uj;
       el = uj;
     } else {
-      const Cons<T, D> up = cell(r - 2, aoff, flip_a);
+      int qp;
+      const T* stp = stage_of(r - 2, qp);
+      const Cons<T, D> up = load(stp, qp, aoff, ghost_l(j + 1), flip_a);
       T chi_v = T(1);
       if (flatten) {
         const T dl = P[2] - P[0];
@@ -346,24 +361,23 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     if (j >= s0) {
       // face (j-1, j), then the update of position j - 1
       Cons<T, D> fj;
-      riemann_q<FLUX>(er_prev, derive(er_prev, gm1), el, derive(el, gm1), S, gamma, gm1, adi,
-                      dtdh, fj, pinf);
+      riemann_qh<FLUX>(er_prev, derive(er_prev, gm1), el, derive(el, gm1), S, gamma, gm1, adi,
+                       dtdh, dhdt, fj, pinf);
       if (j >= s0 + 1) {
         Cons<T, D> res;
 #pragma unroll
         for (int c = 0; c < NC; ++c) res.v[c] = um.v[c] + dtdh * (f_prev.v[c] - fj.v[c]);
-        const int64_t jo = j - 1;  // the updated position
+        const int jo = j - 1;  // the updated position
         if (S == 1) {
           if (owned) {
-            T* out = static_cast<T*>(p.out);
-            const int64_t gi = jo * na + ai;
+            T* o = out + (int64_t)jo * na + ai;
 #pragma unroll
-            for (int c = 0; c < NC; ++c) out[c * pitch + gi] = res.v[c];
+            for (int c = 0; c < NC; ++c) o[c * pitch] = res.v[c];
           }
         } else {
           // collect the column in the output tile; store it when complete
-          const int col = (int)((jo - s0) % Cf::CB);
-          const int buf = (int)(((jo - s0) / Cf::CB) & 1);
+          const int col = (jo - s0) % Cf::CB;
+          const int buf = ((jo - s0) / Cf::CB) & 1;
           T* ob = sm.out + (size_t)buf * Cf::OUT;
           if (col == 0) {
             // the store that last read this tile has finished reading it
@@ -376,7 +390,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
-              tma_store_3d(tout, ob, (int)(jo - (Cf::CB - 1)), (int)a0, 0);
+              tma_store_3d(tout, ob, jo - (Cf::CB - 1), a0, 0);
               bulk_commit();
             }
           }
@@ -413,6 +427,7 @@ __global__ void __launch_bounds__(StagedCfg<T, S>::THREADS, StagedCfg<T, S>::MIN
     p.walk_next[1 - p.walk_slot] = 0u;
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
   const T dtdh = (p.ctrl != nullptr) ? (T)p.ctrl->dtdh : (T)p.dtdh;
+  const T dhdt = T(1.0) / dtdh;  // Lax-Friedrichs coefficient, once per launch
   extern __shared__ __align__(128) unsigned char staged_smem[];
   __shared__ double s_red[Cf::WARPS];
   const int warp = threadIdx.x >> 5;
@@ -441,8 +456,8 @@ __global__ void __launch_bounds__(StagedCfg<T, S>::THREADS, StagedCfg<T, S>::MIN
     item = (int64_t)__shfl_sync(0xffffffffu, v, 0);
   }
   while (item < items && !fault) {
-    staged_strip<T, S, FLUX>(p, &tin, &tout, sm, dtdh, item % nab, (item / nab) * ry, ry,
-                             ws_local, want_ws, gstage, fault);
+    staged_strip<T, S, FLUX>(p, &tin, &tout, sm, dtdh, dhdt, (int)(item % nab),
+                             (int)((item / nab) * ry), ry, ws_local, want_ws, gstage, fault);
     if (next == nullptr) break;
     unsigned int v = 0u;
     if (lane == 0) v = atomicAdd(next, 1u);

@@ -159,13 +159,11 @@ def test_staged_schedules_agree_bitwise(cuda, dtype, shape):
     assert torch.equal(out, x)
 
 
-def _subset_in_subprocess(mode):
+def _subset_in_subprocess(mode, path, select):
     env = dict(os.environ, FLUIDITY_B200_SWEEP=mode)
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
-                        os.path.join(ROOT, "tests", "test_split_gpu.py"), "-k",
-                        "quadrant_2d_per_step or (policy_sweeps and 2d) or loop_matches_host",
-                        "-m", "gpu"], cwd=ROOT, env=env, capture_output=True, text=True,
-                       timeout=900)
+                        os.path.join(ROOT, "tests", path), "-k", select, "-m", "gpu"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
     assert " passed" in r.stdout
 
@@ -175,4 +173,13 @@ def test_older_2d_kernels_parity_subset(cuda, mode):
     """The register walk and the shared-memory tile kernel stay selectable
     (FLUIDITY_B200_SWEEP=walk|tile, read once per process): the 2-D parity
     subset of test_split_gpu.py in a process of its own."""
-    _subset_in_subprocess(mode)
+    _subset_in_subprocess(mode, "test_split_gpu.py",
+                          "quadrant_2d_per_step or (policy_sweeps and 2d) or loop_matches_host")
+
+
+def test_staged_x_sweep_parity_subset(cuda):
+    """FLUIDITY_B200_SWEEP=staged also takes the transposed staged walk for
+    the x sweep: this file's parity cases (not this test) in a process of
+    its own."""
+    _subset_in_subprocess("staged", "test_staged_gpu.py",
+                          "not subset and not older_2d and not schedules")
