@@ -128,8 +128,11 @@ def test_staged_quadrant_white_noise_and_stiff(cuda, oracle, dtype):
 def test_staged_schedules_agree_bitwise(cuda, dtype, shape):
     """The device-resident loop takes strips dynamically from the strip
     counters (shortened strips where the grid is small); fl_split_solve takes
-    one strip per warp.  Both run the same strip code, so two steps agree bit
-    for bit in both dtypes."""
+    one strip per warp.  The staged walk runs the same strip code for both,
+    so where both sweeps are staged (FLUIDITY_B200_SWEEP=staged) two steps
+    agree bit for bit in both dtypes.  By default the x sweep is the register
+    walk, whose two schedules are separately inlined copies that the compiler
+    contracts differently in FP32: there FP32 agrees to rounding."""
     import torch
     from fluidity_b200.solver import Simulation, SplitSolver
     from fluidity_b200.workloads import riemann_states
@@ -156,7 +159,11 @@ def test_staged_schedules_agree_bitwise(cuda, dtype, shape):
         _, x = s.solve(x, y, dtdh, max_ws=mws)
         ws = mws.item()
     torch.cuda.synchronize()
-    assert torch.equal(out, x)
+    if dtype == "f64" or os.environ.get("FLUIDITY_B200_SWEEP") == "staged":
+        assert torch.equal(out, x)
+    else:
+        d = (out.double() - x.double()).abs()
+        assert (d / x.double().abs().clamp_min(1.0)).max().item() < 1e-5
 
 
 def _subset_in_subprocess(mode, path, select):
@@ -181,5 +188,4 @@ def test_staged_x_sweep_parity_subset(cuda):
     """FLUIDITY_B200_SWEEP=staged also takes the transposed staged walk for
     the x sweep: this file's parity cases (not this test) in a process of
     its own."""
-    _subset_in_subprocess("staged", "test_staged_gpu.py",
-                          "not subset and not older_2d and not schedules")
+    _subset_in_subprocess("staged", "test_staged_gpu.py", "not subset and not older_2d")
