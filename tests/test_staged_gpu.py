@@ -5,7 +5,10 @@ The staged kernel runs wherever a state's rows and planes are multiples of 16
 bytes (x extent a multiple of 2 in FP64, of 4 in FP32); these shapes are
 chosen so that it does, in both dtypes: partial warps across the sweep (x or y
 extents not multiples of 32), strips shorter than the walk's reach, the
-smallest grids the ABI accepts, reflective ends and every policy.
+smallest grids the ABI accepts, reflective ends and every policy.  By default
+it takes the FP64 y sweep; test_staged_x_sweep_parity_subset reruns this
+file's parity cases with FLUIDITY_B200_SWEEP=staged, where it takes both
+sweeps in both dtypes.
 
 Bars per sweep as in test_split_gpu.py: FP64 1e-12 relative per cell (floor
 1e-3 of the component's magnitude), FP32 1e-5 of the component's magnitude.
