@@ -89,6 +89,24 @@ def workload_config(a):
     }
 
 
+def alternating_transposes(a):
+    """Plane transposes per run of the device-resident loop: the FP64 2-D loop
+    alternates layouts (state in, then back out) when both extents are
+    multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set; "staged"
+    extends it to FP32."""
+    mode = os.environ.get("FLUIDITY_B200_SWEEP", "")
+    elem = 8 if a.dtype == "f64" else 4
+    on = (mode == "staged") or (mode == "" and a.dtype == "f64")
+    return 2 if on and (a.size * elem) % 16 == 0 else 0
+
+
+def sweep_kernel_name(a):
+    if alternating_transposes(a):
+        return ("staged_walk_2d (x and y sweeps, averaged; each sweep reads its input with "
+                "its own dimension slowest and writes it transposed)")
+    return "walk_kernel_2d (x and y sweeps, averaged)"
+
+
 # ---- distributed plumbing ---------------------------------------------------
 
 def dist_init(a):
@@ -382,14 +400,14 @@ def run_ours(a, world, rank, local):
                                  if (a.dtype, a.flux) in MEASURED_TRAFFIC_PER_CELL else None),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
                                        "2048^2 capture, per cell, scaled to this grid",
-                     "kernel": "walk_kernel_2d (x and y sweeps, averaged)",
+                     "kernel": sweep_kernel_name(a),
                      "algorithmic_bytes_per_launch": bytes_per_sweep,
                      "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "steps": e2e_steps, "api": "fl_host_pipe_run (pinned host in/out)",
                 "overlap": "upload of step k+1 and download of step k-1 run during step k"},
-        "gpu_launches": a.steps * (3 + launches_per_run),
+        "gpu_launches": a.steps * (3 + launches_per_run + alternating_transposes(a)),
         "clocks": clocks,
     }
     if headline_checks is not None:

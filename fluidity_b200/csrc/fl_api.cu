@@ -257,6 +257,43 @@ __global__ void finalize_kernel(StepControl* c, unsigned long long* word, int ad
   }
 }
 
+// Transposes every component plane of a 2-D state: plane c of `in` holds
+// ns rows of nf cells (nf fastest), plane c of `out` receives nf rows of ns
+// cells; planes are `pitch` elements apart in both.  32 x 32 tiles through
+// shared memory, so that both the loads and the stores are coalesced.
+template <typename T>
+__global__ void __launch_bounds__(256) transpose_planes_kernel(const T* __restrict__ in,
+                                                               T* __restrict__ out, int64_t pitch,
+                                                               int64_t nf, int64_t ns) {
+  __shared__ T tile[32][33];
+  const T* src = in + (int64_t)blockIdx.z * pitch;
+  T* dst = out + (int64_t)blockIdx.z * pitch;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t f0 = (int64_t)blockIdx.x * 32;
+  for (int64_t s0 = (int64_t)blockIdx.y * 32; s0 < ns; s0 += (int64_t)gridDim.y * 32) {
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t sr = s0 + i, f = f0 + tx;
+      if (sr < ns && f < nf) tile[i][tx] = src[sr * nf + f];
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t f = f0 + i, sr = s0 + tx;
+      if (f < nf && sr < ns) dst[f * ns + sr] = tile[tx][i];
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+cudaError_t launch_transpose(const void* in, void* out, int64_t pitch, int64_t nf, int64_t ns,
+                             cudaStream_t st) {
+  const int64_t gy = (ns + 31) / 32;
+  const dim3 grid((unsigned)((nf + 31) / 32), (unsigned)(gy < 65535 ? gy : 65535), 4);
+  transpose_planes_kernel<T><<<grid, dim3(32, 8), 0, st>>>(static_cast<const T*>(in),
+                                                          static_cast<T*>(out), pitch, nf, ns);
+  return cudaGetLastError();
+}
+
 __global__ void init_control_kernel(StepControl* c, double cfl, double res, double sim_time,
                                     long long max_iters, int is_f32) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -608,6 +645,45 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
   p.ws_lo = sim->own_lo;
   p.ws_hi = sim->own_hi;
   p.scratch = sim->scratch;
+  p.status = &sim->ctrl->status;
+  if (D == 2 && nsteps > 0) {
+    // The layout-alternating loop: the state goes from buffer a (x fastest)
+    // into buffer b with y fastest; each x sweep reads b and writes a (x
+    // fastest), each y sweep reads a and writes b (y fastest), so that both
+    // sweeps walk along their input's slow dimension; after the last step
+    // buffer a receives the state in the caller's layout again.
+    SweepParams probe = p;
+    probe.in = sim->a;
+    probe.out = sim->b;
+    const bool tl = sim->pol.f32 ? loop_transposes_f32(probe) : loop_transposes_f64(probe);
+    if (tl) {
+      const int64_t n0 = sim->grid.n[0], n1 = sim->grid.n[1], pt = sim->grid.pitch;
+      cudaError_t e = sim->pol.f32 ? launch_transpose<float>(sim->a, sim->b, pt, n0, n1, st)
+                                   : launch_transpose<double>(sim->a, sim->b, pt, n0, n1, st);
+      if (e != cudaSuccess) return cuda_fail(e, "fl_sim_steps");
+      p.transposed = 1;
+      for (int64_t k = 0; k < nsteps; ++k) {
+        for (int d = 0; d < 2; ++d) {
+          p.in = (d == 0) ? sim->b : sim->a;
+          p.out = (d == 0) ? sim->a : sim->b;
+          p.walk_next = sim->ctrl->walk_next;
+          p.walk_slot = (int)((sim->enqueued * 2 + d) & 1);
+          p.ws_accum = (d == 1) ? &sim->ctrl->ws_bits : nullptr;
+          p.finalize = (d == 1) ? 1 : 0;
+          e = launch_sweep(p, sim->pol, 2, d, st);
+          if (e != cudaSuccess) {
+            sim->counters_dirty = 1;
+            return cuda_fail(e, "fl_sim_steps");
+          }
+        }
+        sim->enqueued += 1;
+      }
+      e = sim->pol.f32 ? launch_transpose<float>(sim->b, sim->a, pt, n1, n0, st)
+                       : launch_transpose<double>(sim->b, sim->a, pt, n1, n0, st);
+      if (e != cudaSuccess) return cuda_fail(e, "fl_sim_steps");
+      return kOk;
+    }
+  }
   for (int64_t k = 0; k < nsteps; ++k) {
     // input of this step: for even D the state returns to buffer a every
     // step; for odd D it alternates a, b, a, ...
@@ -693,6 +769,7 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   p.scratch = sim->scratch;
   p.walk_next = sim->ctrl->walk_next;
   p.walk_slot = (int)((sim->enqueued * D + dim) & 1);
+  p.status = &sim->ctrl->status;
   p.in = si;
   p.out = so;
   const bool last = (dim == D - 1);
@@ -737,6 +814,9 @@ int fl_sim_status(fl_sim* sim, void* stream, int64_t* iters, double* run_time, i
     *result = in_b ? sim->b : sim->a;
   }
   if (h.status == kENan) return fail(kENan, "non-finite wavespeed after step %lld", (long long)h.iters);
+  if (h.status == kETimeout)
+    return fail(kETimeout, "a sweep's wait for its staged copies gave up after step %lld",
+                (long long)h.iters);
   return kOk;
 }
 

@@ -62,6 +62,11 @@ struct SweepParams {
   // nullable: a kernel whose bounded wait on its own copies gave up writes
   // kETimeout here (and stops the loop through ctrl->done when ctrl is set)
   int* status;
+  // 2-D only, 1: the sweep of the layout-alternating loop.  `in` holds the
+  // state with the sweep dimension slowest (x sweep: y fastest; y sweep:
+  // x fastest) and `out` receives it transposed (x sweep: x fastest; y
+  // sweep: y fastest).  Both layouts keep the planes `pitch` apart.
+  int transposed;
 };
 
 // Tensor map of one SoA state buffer for the TMA-staged sweeps: a 3-D

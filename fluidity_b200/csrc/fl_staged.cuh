@@ -45,23 +45,31 @@
 
 namespace fl {
 
-template <typename T, int S>
+// GEO = 1: the walk runs along the slow dimension of the input's layout and a
+// stage is one row of 40 cells along its fast dimension (the lanes' 32 plus 4
+// on each side).  GEO = 0: the walk runs along the fast dimension and a stage
+// is 16 bytes of it (2 cells in FP64, 4 in FP32) over 38 rows (the lanes' 32
+// plus 3 on each side).  TOUT: updated cells collect in a shared tile of 16
+// bytes along the walk by 32 lanes, written back by a TMA store whose tensor
+// map has the walk dimension fastest; otherwise each lane stores its cell,
+// in the input's layout.
+template <typename T, int GEO, bool TOUT>
 struct StagedCfg {
   static constexpr int NC = 4;
-  static constexpr int CB = 16 / (int)sizeof(T);  // x sweep: columns per stage
-  static constexpr int PPS = (S == 0) ? CB : 1;    // walk positions per stage
-  static constexpr int BW = (S == 1) ? 40 : 38;    // across extent of a box
-  static constexpr int AOFF = (S == 1) ? 4 : 3;    // box index of lane 0's cell
+  static constexpr int CB = 16 / (int)sizeof(T);  // cells per 16 bytes
+  static constexpr int PPS = GEO ? 1 : CB;         // walk positions per stage
+  static constexpr int BW = GEO ? 40 : 38;         // across extent of a box
+  static constexpr int AOFF = GEO ? 4 : 3;         // box index of lane 0's cell
   static constexpr int STAGE = NC * BW * PPS;      // elements per stage
   static constexpr uint32_t STAGE_BYTES = STAGE * sizeof(T);
   // stages the walk reads at once (positions k-4 .. k), plus prefetch
-  static constexpr int LIVE = (S == 1) ? 5 : (CB == 2 ? 3 : 2);
-  static constexpr int NS = (S == 1) ? 8 : (sizeof(T) == 8 ? 5 : 4);
-  static constexpr int WARPS = (S == 0 && sizeof(T) == 8) ? 2 : 4;
+  static constexpr int LIVE = GEO ? 5 : (CB == 2 ? 3 : 2);
+  static constexpr int NS = GEO ? 8 : (sizeof(T) == 8 ? 5 : 4);
+  static constexpr int WARPS = (!GEO && sizeof(T) == 8) ? 2 : 4;
   static constexpr int THREADS = 32 * WARPS;
   static constexpr int RY = FL_STAGED_RY;
-  static constexpr int OUT = (S == 0) ? NC * 32 * CB : 0;  // output tile elements
-  static constexpr int NOUT = (S == 0) ? 2 : 0;              // output tiles (double buffer)
+  static constexpr int OUT = TOUT ? NC * 32 * CB : 0;  // output tile elements
+  static constexpr int NOUT = TOUT ? 2 : 0;            // output tiles (double buffer)
   static constexpr size_t RING_BYTES = (size_t)NS * STAGE_BYTES;
   static constexpr size_t OUT_BYTES = (size_t)NOUT * OUT * sizeof(T);
   static constexpr size_t X_BYTES = 3 * 40 * sizeof(T);
@@ -73,14 +81,14 @@ struct StagedCfg {
   static constexpr size_t SMEM = WARPS * WARP_BYTES + 128;
   static_assert(STAGE_BYTES % 128 == 0 && (OUT * sizeof(T)) % 128 == 0, "128-byte boxes");
   // registers held to this many resident CTAs per SM
-  static constexpr int MIN_CTAS = (sizeof(T) == 8) ? (S == 0 ? 7 : 4) : (S == 0 ? 4 : 6);
+  static constexpr int MIN_CTAS = (sizeof(T) == 8) ? (GEO ? 4 : 7) : (GEO ? 6 : 4);
   static_assert(NS >= LIVE + 1, "the ring needs room to prefetch");
 };
 
 // Per-warp view of the shared-memory region.
-template <typename T, int S>
+template <typename T, int GEO, bool TOUT>
 struct StagedSmem {
-  using C = StagedCfg<T, S>;
+  using C = StagedCfg<T, GEO, TOUT>;
   T* ring;
   T* out;
   T* xp;   // pressure across the warp, by box index
@@ -99,11 +107,11 @@ struct StagedSmem {
 
 // Box coordinate along the sweep of stage t's first position p0, and whether
 // the stage is a mirror image (its positions map to columns in reverse).
-template <typename T, int S>
+template <typename T, int GEO, bool TOUT>
 __device__ __forceinline__ int stage_along(int p0, int nl, bool& reversed) {
-  using C = StagedCfg<T, S>;
+  using C = StagedCfg<T, GEO, TOUT>;
   reversed = false;
-  if (S == 1) {  // one row per stage: the mirrored row itself
+  if (GEO) {  // one row per stage: the mirrored row itself
     bool f;
     return (int)mirror_index((int64_t)p0, (int64_t)nl, f);
   }
@@ -118,28 +126,19 @@ __device__ __forceinline__ int stage_along(int p0, int nl, bool& reversed) {
   return p0;
 }
 
-template <typename T, int S>
-__device__ __forceinline__ void stage_issue(const StagedSmem<T, S>& sm, const CUtensorMap* tin,
-                                            int slot, int p0, int nl, int a0) {
-  using C = StagedCfg<T, S>;
+template <typename T, int GEO, bool TOUT>
+__device__ __forceinline__ void stage_issue(const StagedSmem<T, GEO, TOUT>& sm,
+                                            const CUtensorMap* tin, int slot, int p0, int nl,
+                                            int a0) {
+  using C = StagedCfg<T, GEO, TOUT>;
   bool rev;
-  const int al = stage_along<T, S>(p0, nl, rev);
+  const int al = stage_along<T, GEO, TOUT>(p0, nl, rev);
   T* dst = sm.ring + (size_t)slot * C::STAGE;
   mbar_expect_tx(&sm.bars[slot], C::STAGE_BYTES);
-  if (S == 1)
+  if (GEO)
     tma_load_3d(dst, tin, &sm.bars[slot], a0 - C::AOFF, al, 0);
   else
     tma_load_3d(dst, tin, &sm.bars[slot], al, a0 - C::AOFF, 0);
-}
-
-// Component c of the cell at box index `a` of the stage in `slot`, walk
-// position offset q within the stage.
-template <typename T, int S>
-__device__ __forceinline__ T stage_at(const StagedSmem<T, S>& sm, int slot, int q, int a, int c) {
-  using C = StagedCfg<T, S>;
-  const T* st = sm.ring + (size_t)slot * C::STAGE;
-  if (S == 1) return st[c * C::BW + a];
-  return st[(c * C::BW + a) * C::CB + q];
 }
 
 // One warp's strip: across block `ab` (cells a0 = 32 ab .. a0 + 31 across
@@ -147,13 +146,14 @@ __device__ __forceinline__ T stage_at(const StagedSmem<T, S>& sm, int slot, int 
 // folds the wavespeed of each stored cell into ws_local.  gstage counts the
 // stages this warp has issued before (ring slot and barrier phase).  Grid
 // extents are below 2^30 (checked by the launcher), so positions are ints.
-template <typename T, int S, int FLUX>
+template <typename T, int S, int FLUX, int GEO, bool TOUT>
 __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtensorMap* tin,
                                              const CUtensorMap* tout,
-                                             const StagedSmem<T, S>& sm, T dtdh, T dhdt, int ab,
+                                             const StagedSmem<T, GEO, TOUT>& sm, T dtdh, T dhdt,
+                                             int ab,
                                              int s0, int ry, double& ws_local, bool want_ws,
                                              uint32_t& gstage, int& fault) {
-  using Cf = StagedCfg<T, S>;
+  using Cf = StagedCfg<T, GEO, TOUT>;
   constexpr int D = 2;
   constexpr int NC = 4;
   constexpr int PPS = Cf::PPS;
@@ -207,16 +207,16 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   if (lane == 0) {
     fence_proxy_async_smem();
     for (int t = 0; t < issued; ++t)
-      stage_issue<T, S>(sm, tin, (int)((g0 + t) % NS), k_first + t * PPS, nl, a0);
+      stage_issue<T, GEO, TOUT>(sm, tin, (int)((g0 + t) % NS), k_first + t * PPS, nl, a0);
   }
 
   // the stage holding walk offset r, and r's column within it
   auto stage_of = [&](int r, int& q) -> const T* {
     const int t = r / PPS;
     q = r - t * PPS;
-    if (S == 0) {
+    if (!GEO) {
       bool rev;
-      (void)stage_along<T, S>(k_first + t * PPS, nl, rev);
+      (void)stage_along<T, GEO, TOUT>(k_first + t * PPS, nl, rev);
       if (rev) q = PPS - 1 - q;
     }
     return sm.ring + (size_t)((g0 + t) % NS) * Cf::STAGE;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     Cons<T, D> u;
 #pragma unroll
     for (int c = 0; c < NC; ++c)
-      u.v[c] = (S == 1) ? st[c * Cf::BW + a] : st[(c * Cf::BW + a) * Cf::CB + q];
+      u.v[c] = GEO ? st[c * Cf::BW + a] : st[(c * Cf::BW + a) * Cf::CB + q];
     if (gl) u.v[2 + S] = (-(u.v[2 + S] / u.v[0])) * u.v[0];
     if (fx) u.v[3 - S] = (-(u.v[3 - S] / u.v[0])) * u.v[0];
     return u;
@@ -258,7 +258,8 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
         __syncwarp();
         if (lane == 0) {
           fence_proxy_async_smem();
-          stage_issue<T, S>(sm, tin, (int)((g0 + td) % NS), k_first + (td + NS) * PPS, nl, a0);
+          stage_issue<T, GEO, TOUT>(sm, tin, (int)((g0 + td) % NS), k_first + (td + NS) * PPS,
+                                    nl, a0);
         }
         ++issued;
       }
@@ -368,7 +369,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
 #pragma unroll
         for (int c = 0; c < NC; ++c) res.v[c] = um.v[c] + dtdh * (f_prev.v[c] - fj.v[c]);
         const int jo = j - 1;  // the updated position
-        if (S == 1) {
+        if (!TOUT) {
           if (owned) {
             T* o = out + (int64_t)jo * na + ai;
 #pragma unroll
@@ -418,11 +419,12 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
 // take strips, across block fastest, from walk_next[walk_slot] until none is
 // left.  The sweep clears the other counter, which the next sweep of the
 // stream uses.  Both schedules run the same strip code.
-template <typename T, int S, int FLUX>
-__global__ void __launch_bounds__(StagedCfg<T, S>::THREADS, StagedCfg<T, S>::MIN_CTAS)
+template <typename T, int S, int FLUX, int GEO, bool TOUT>
+__global__ void __launch_bounds__(StagedCfg<T, GEO, TOUT>::THREADS,
+                                  StagedCfg<T, GEO, TOUT>::MIN_CTAS)
     staged_walk_2d(SweepParams p, const __grid_constant__ CUtensorMap tin,
                    const __grid_constant__ CUtensorMap tout) {
-  using Cf = StagedCfg<T, S>;
+  using Cf = StagedCfg<T, GEO, TOUT>;
   if (p.walk_next != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
     p.walk_next[1 - p.walk_slot] = 0u;
   if (p.ctrl != nullptr && *(volatile int*)&p.ctrl->done) return;
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(StagedCfg<T, S>::THREADS, StagedCfg<T, S>::MIN
   const int lane = threadIdx.x & 31;
   const uint32_t mis = smem_addr(staged_smem) & 127u;
   unsigned char* base = staged_smem + (mis ? 128u - mis : 0u);
-  StagedSmem<T, S> sm(base + (size_t)warp * Cf::WARP_BYTES);
+  StagedSmem<T, GEO, TOUT> sm(base + (size_t)warp * Cf::WARP_BYTES);
   if (lane == 0) {
     for (int s = 0; s < Cf::NS; ++s) mbar_init(&sm.bars[s], 1);
     mbar_init_fence();
@@ -456,14 +458,14 @@ __global__ void __launch_bounds__(StagedCfg<T, S>::THREADS, StagedCfg<T, S>::MIN
     item = (int64_t)__shfl_sync(0xffffffffu, v, 0);
   }
   while (item < items && !fault) {
-    staged_strip<T, S, FLUX>(p, &tin, &tout, sm, dtdh, dhdt, (int)(item % nab),
+    staged_strip<T, S, FLUX, GEO, TOUT>(p, &tin, &tout, sm, dtdh, dhdt, (int)(item % nab),
                              (int)((item / nab) * ry), ry, ws_local, want_ws, gstage, fault);
     if (next == nullptr) break;
     unsigned int v = 0u;
     if (lane == 0) v = atomicAdd(next, 1u);
     item = (int64_t)__shfl_sync(0xffffffffu, v, 0);
   }
-  if (S == 0 && lane == 0) bulk_wait<0>();
+  if (TOUT && lane == 0) bulk_wait<0>();
   if (fault && lane == 0 && p.status != nullptr) {
     atomicExch(p.status, kETimeout);
     if (p.ctrl != nullptr) atomicExch(&p.ctrl->done, 1);

@@ -488,12 +488,14 @@ def test_dynamic_strips_equal_static_grid(cuda, dtype, shape):
     """The device-resident loop takes its strips dynamically (64-row strips
     at 2048^2, shortened to 32 rows where 64-row strips cannot fill the
     GPU); fl_split_solve launches the static grid.  Two steps of each, with
-    the loop's own time steps replayed on the static path, agree bit for
-    bit in FP64: the schedule decides only which warp computes a cell.  The
-    two schedules are separately inlined copies of the strip code (one call
-    site for both measured 6-11% slower), and in FP32 the compiler's
-    contractions differ between the copies by a few ulps (6e-7 relative
-    measured), so FP32 agrees to rounding."""
+    the loop's own time steps replayed on the static path.  With the
+    register walk for both (FLUIDITY_B200_SWEEP=walk) they agree bit for
+    bit in FP64: the schedule decides only which warp computes a cell; the
+    walk's two schedules are separately inlined copies of the strip code,
+    which the compiler contracts differently in FP32 (6e-7 relative
+    measured).  By default the FP64 loop alternates layouts and sweeps x
+    with the staged walk while fl_split_solve sweeps x with the register
+    walk: there the two agree to the FP64 parity bar."""
     import torch
     from fluidity_b200.solver import Simulation, SplitSolver
     from fluidity_b200.workloads import riemann_states
@@ -522,8 +524,10 @@ def test_dynamic_strips_equal_static_grid(cuda, dtype, shape):
         _, x = s.solve(x, y, dtdh, max_ws=mws)      # 2-D: the result returns to x
         ws = mws.item()
     torch.cuda.synchronize()
-    if dtype == "f64":
+    if dtype == "f64" and os.environ.get("FLUIDITY_B200_SWEEP") == "walk":
         assert torch.equal(out, x)
+    elif dtype == "f64":
+        assert rel_err(out.cpu().numpy(), x.cpu().numpy()) < TOL["f64"]
     else:
         d = (out.double() - x.double()).abs()
         worst = (d / x.double().abs().clamp_min(1.0)).max().item()
