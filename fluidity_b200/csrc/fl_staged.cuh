@@ -69,7 +69,9 @@ struct StagedCfg {
   static constexpr int THREADS = 32 * WARPS;
   static constexpr int RY = FL_STAGED_RY;
   static constexpr int OUT = TOUT ? NC * 32 * CB : 0;  // output tile elements
-  static constexpr int NOUT = TOUT ? 2 : 0;            // output tiles (double buffer)
+  // output tiles: one for the row geometry (a second would cost a resident
+  // CTA per SM in FP64: 61.6 KB instead of 53.4 KB per CTA), two otherwise
+  static constexpr int NOUT = TOUT ? (GEO ? 1 : 2) : 0;
   static constexpr size_t RING_BYTES = (size_t)NS * STAGE_BYTES;
   static constexpr size_t OUT_BYTES = (size_t)NOUT * OUT * sizeof(T);
   static constexpr size_t X_BYTES = 3 * 40 * sizeof(T);
@@ -378,11 +380,16 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
         } else {
           // collect the column in the output tile; store it when complete
           const int col = (jo - s0) % Cf::CB;
-          const int buf = ((jo - s0) / Cf::CB) & 1;
+          const int buf = (Cf::NOUT == 2) ? ((jo - s0) / Cf::CB) & 1 : 0;
           T* ob = sm.out + (size_t)buf * Cf::OUT;
           if (col == 0) {
             // the store that last read this tile has finished reading it
-            if (lane == 0) bulk_wait_read<1>();
+            if (lane == 0) {
+              if (Cf::NOUT == 2)
+                bulk_wait_read<1>();
+              else
+                bulk_wait_read<0>();
+            }
             __syncwarp();
           }
 #pragma unroll
