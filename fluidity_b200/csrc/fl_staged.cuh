@@ -64,13 +64,19 @@ struct StagedCfg {
   static constexpr uint32_t STAGE_BYTES = STAGE * sizeof(T);
   // stages the walk reads at once (positions k-4 .. k), plus prefetch
   static constexpr int LIVE = GEO ? 5 : (CB == 2 ? 3 : 2);
-  static constexpr int NS = GEO ? 8 : (sizeof(T) == 8 ? 5 : 4);
+  // FP64 rows with a tiled output: 7 stages, so that four CTAs stay resident
+  static constexpr int NS = GEO ? ((TOUT && sizeof(T) == 8) ? 7 : 8) : (sizeof(T) == 8 ? 5 : 4);
   static constexpr int WARPS = (!GEO && sizeof(T) == 8) ? 2 : 4;
   static constexpr int THREADS = 32 * WARPS;
   static constexpr int RY = FL_STAGED_RY;
-  static constexpr int OUT = TOUT ? NC * 32 * CB : 0;  // output tile elements
+  // A tiled output collects 32 bytes along the walk per lane (one DRAM
+  // sector: 4 cells in FP64, 8 in FP32) before its TMA store; 16-byte
+  // stores left half-written sectors that L2 filled from DRAM, 55% more
+  // reads than the sweep's own.
+  static constexpr int OPS = 32 / (int)sizeof(T);      // walk positions per store
+  static constexpr int OUT = TOUT ? NC * 32 * OPS : 0;  // output tile elements
   // output tiles: one for the row geometry (a second would cost a resident
-  // CTA per SM in FP64: 61.6 KB instead of 53.4 KB per CTA), two otherwise
+  // CTA per SM in FP64), two otherwise
   static constexpr int NOUT = TOUT ? (GEO ? 1 : 2) : 0;
   static constexpr size_t RING_BYTES = (size_t)NS * STAGE_BYTES;
   static constexpr size_t OUT_BYTES = (size_t)NOUT * OUT * sizeof(T);
@@ -379,8 +385,8 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
           }
         } else {
           // collect the column in the output tile; store it when complete
-          const int col = (jo - s0) % Cf::CB;
-          const int buf = (Cf::NOUT == 2) ? ((jo - s0) / Cf::CB) & 1 : 0;
+          const int col = (jo - s0) % Cf::OPS;
+          const int buf = (Cf::NOUT == 2) ? ((jo - s0) / Cf::OPS) & 1 : 0;
           T* ob = sm.out + (size_t)buf * Cf::OUT;
           if (col == 0) {
             // the store that last read this tile has finished reading it
@@ -393,12 +399,14 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
             __syncwarp();
           }
 #pragma unroll
-          for (int c = 0; c < NC; ++c) ob[(c * 32 + lane) * Cf::CB + col] = res.v[c];
-          if (col == Cf::CB - 1) {
+          for (int c = 0; c < NC; ++c) ob[(c * 32 + lane) * Cf::OPS + col] = res.v[c];
+          // the group is complete, or the strip ends (a partial group only
+          // at the domain's end, where the store is cut at the extent)
+          if (col == Cf::OPS - 1 || jo == s_end - 1) {
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
-              tma_store_3d(tout, ob, jo - (Cf::CB - 1), a0, 0);
+              tma_store_3d(tout, ob, jo - col, a0, 0);
               bulk_commit();
             }
           }
