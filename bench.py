@@ -38,11 +38,12 @@ sys.path.insert(0, ROOT)
 
 GAMMA = 1.4
 SEED = 0
-# DRAM bytes (read + write) per cell of one sweep launch, from the ncu
-# capture of the 2048^2 FP64 HLLC case (walk_kernel_2d, x and y sweeps
-# averaged: 241.5 MB per launch over 2048^2 cells); traffic grows with the
-# cell count, so the bench scales it to its own grid.
-MEASURED_TRAFFIC_PER_CELL = {("f64", "hllc"): 57.6}
+# DRAM bytes (read + write) per cell of one sweep launch, measured by ncu at
+# 4096^2 on four consecutive launches of the headline loop (FP64 HLLC,
+# staged_walk_2d x and y sweeps of the alternating-layout loop: 602.2 MB read
+# + 494.5 MB written per launch on average, 1,096.7 MB against 1,073.7 MB
+# algorithmic; profiles/staged_walk_2d_f64_hllc_4096sq_launches.md).
+MEASURED_TRAFFIC_PER_CELL = {("f64", "hllc"): 1096.7e6 / 4096 ** 2}
 
 
 def parse():
@@ -398,8 +399,9 @@ def run_ours(a, world, rank, local):
                      "frac": achieved / peak,
                      "traffic": (MEASURED_TRAFFIC_PER_CELL[(a.dtype, a.flux)] * cells
                                  if (a.dtype, a.flux) in MEASURED_TRAFFIC_PER_CELL else None),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
-                                       "2048^2 capture, per cell, scaled to this grid",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                       "average over 4 sweep launches of the 4096^2 loop, "
+                                       "per cell (scaled to this grid when it differs)",
                      "kernel": sweep_kernel_name(a),
                      "algorithmic_bytes_per_launch": bytes_per_sweep,
                      "launch_ms": sweep_s * 1e3, "peak_source": peak_src},
