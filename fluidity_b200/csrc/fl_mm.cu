@@ -124,7 +124,13 @@ __device__ void star_left(const double* ul, const double* ur, double gl, double 
   out[1] = scale * (ul[1] + ul[0] * (s_star - vl) * (s_star + pl / (ul[0] * sf)));
 }
 
-// bilinear probe around (x, y) with offsets w in cells (math/interp.hpp:88-104)
+// Probe of the state around (x, y) with offsets w in cells, with the
+// arithmetic of the reference's 2-D math::interp (math/interp.hpp:120-167)
+// as it computes: X0, X1 the cells offset by off_x and off_x + sign along x
+// from the source, Y0, Y1 those offset along y; close = X0(1-fx) + X1 fx,
+// far = Y0(1-fx) + Y1 fx, r = close(1-fy) + far fy.  (The function's comment
+// documents a bilinear form over the four cells of the offset square, which
+// its code does not compute.)
 template <typename T>
 __device__ void interp2(const T* u, int64_t pitch, int64_t nx, int64_t ny, int64_t x, int64_t y,
                         const double* w, double* out) {
@@ -139,17 +145,17 @@ __device__ void interp2(const T* u, int64_t pitch, int64_t nx, int64_t ny, int64
     off[d] = (int64_t)((double)sg[d] * ao);
     f[d] = aw - ao;
   }
-  double A[4], B[4], Cc[4], Dd[4];
-  load4(u, pitch, midx(nx, ny, x + off[0], y + off[1]), A);
-  load4(u, pitch, midx(nx, ny, x + off[0] + sg[0], y + off[1]), B);
-  load4(u, pitch, midx(nx, ny, x + off[0], y + off[1] + sg[1]), Cc);
-  load4(u, pitch, midx(nx, ny, x + off[0] + sg[0], y + off[1] + sg[1]), Dd);
-  const double fx1 = 1.0 - f[0], fy1 = 1.0 - f[1];
+  double X0[4], X1[4], Y0[4], Y1[4];
+  load4(u, pitch, midx(nx, ny, x + off[0], y), X0);
+  load4(u, pitch, midx(nx, ny, x + off[0] + sg[0], y), X1);
+  load4(u, pitch, midx(nx, ny, x, y + off[1]), Y0);
+  load4(u, pitch, midx(nx, ny, x, y + off[1] + sg[1]), Y1);
+  const double factor = 1.0 - f[0];
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const double x1 = A[c] * fx1 + B[c] * f[0];
-    const double x2 = Cc[c] * fx1 + Dd[c] * f[0];
-    out[c] = x1 * fy1 + x2 * f[1];
+    const double close = X0[c] * factor + X1[c] * f[0];
+    const double far = Y0[c] * factor + Y1[c] * f[0];
+    out[c] = close * (1.0 - f[1]) + far * f[1];
   }
 }
 

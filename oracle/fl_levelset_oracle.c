@@ -9,11 +9,16 @@
  * as boundary::load_padding_with_boundaries does with transmissive bounds
  * (boundary/boundary_loading.hpp:123-175).
  *
- * Parity pin: none against a run of the reference -- its multimaterial driver
- * does not run as shipped (MultimaterialSimulator::simulate is commented out,
+ * Parity pin: the reference's multimaterial driver does not run as shipped
+ * (MultimaterialSimulator::simulate is commented out,
  * simulator/multimaterial_simulator.hpp:656-694, and several of its launches
- * swap grid and block).  The formulas below follow the cited reference lines
- * and the CUDA kernels are checked against this file.
+ * swap grid and block), but its per-cell level-set functors are
+ * __host__ __device__ and run on the host (oracle/ref_driver_ls.cpp).  The
+ * flo_ls_* pieces below -- WENO-HJ5 derivatives, Godunov upwind gradients,
+ * the Hamiltonian, the first two RK3 stages, the local eikonal solve and the
+ * interface-normal velocity -- are pinned bit for bit to them through
+ * tests/golden/levelset.npz (tests/test_levelset_pinned.py).  The CUDA
+ * kernels are checked against this file.
  */
 #include <float.h>
 #include <math.h>
@@ -103,14 +108,11 @@ static double hamiltonian(const double* f, int64_t nx, int64_t ny, int64_t x, in
   return v * sqrt(r);
 }
 
-/* One TVD-RK3 step of phi_t + v |grad phi| = 0
- * (scheme/updaters/runge_kutta_3.hpp:110-148), every stage over the whole
- * grid with freshly mirrored ghosts. */
-void flo_ls_advect_f64(int64_t nx, int64_t ny, const double* phi, const double* vel, double dt,
-                       double h, double* out) {
-  const int64_t n = nx * ny;
-  double* s1 = (double*)malloc(sizeof(double) * n);
-  double* s2 = (double*)malloc(sizeof(double) * n);
+/* The first two TVD-RK3 stages of phi_t + v |grad phi| = 0
+ * (scheme/updaters/runge_kutta_3.hpp:110-148), each over the whole grid with
+ * freshly mirrored ghosts. */
+void flo_ls_rk3_stages_f64(int64_t nx, int64_t ny, const double* phi, const double* vel,
+                           double dt, double h, double* s1, double* s2) {
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
@@ -121,6 +123,16 @@ void flo_ls_advect_f64(int64_t nx, int64_t ny, const double* phi, const double* 
       const int64_t i = y * nx + x;
       s2[i] = 0.75 * phi[i] + 0.25 * (s1[i] - dt * hamiltonian(s1, nx, ny, x, y, h, vel[i]));
     }
+}
+
+/* One TVD-RK3 step: the two stages above, then the third stage and the
+ * final combination (1/3) phi^n + (2/3)(stage 3). */
+void flo_ls_advect_f64(int64_t nx, int64_t ny, const double* phi, const double* vel, double dt,
+                       double h, double* out) {
+  const int64_t n = nx * ny;
+  double* s1 = (double*)malloc(sizeof(double) * n);
+  double* s2 = (double*)malloc(sizeof(double) * n);
+  flo_ls_rk3_stages_f64(nx, ny, phi, vel, dt, h, s1, s2);
   const double f13 = 1.0 / 3.0, f23 = 2.0 * f13;
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
@@ -186,6 +198,44 @@ static double eik_local(const double* d, int64_t nx, int64_t ny, int64_t x, int6
 }
 
 static int sgn(double v) { return (0.0 < v) - (v < 0.0); }
+
+/* ---- per-cell pieces, exported for the pin against the reference ------- */
+
+/* WENO-HJ5 one-sided derivatives: back[d * n + i], fwrd[d * n + i]. */
+void flo_ls_weno_f64(int64_t nx, int64_t ny, const double* phi, double h, double* back,
+                     double* fwrd) {
+  const int64_t n = nx * ny;
+  for (int64_t y = 0; y < ny; ++y)
+    for (int64_t x = 0; x < nx; ++x)
+      for (int d = 0; d < 2; ++d) {
+        back[d * n + y * nx + x] = weno_back(phi, nx, ny, x, y, d, h);
+        fwrd[d * n + y * nx + x] = weno_fwrd(phi, nx, ny, x, y, d, h);
+      }
+}
+
+/* Godunov upwind |grad phi|: the branch for v <= 0 (fwd) and v > 0 (bwd). */
+void flo_ls_godunov_f64(int64_t nx, int64_t ny, const double* phi, double h, double* fwd,
+                        double* bwd) {
+  for (int64_t y = 0; y < ny; ++y)
+    for (int64_t x = 0; x < nx; ++x) {
+      fwd[y * nx + x] = hamiltonian(phi, nx, ny, x, y, h, -1.0) / -1.0;
+      bwd[y * nx + x] = hamiltonian(phi, nx, ny, x, y, h, 1.0);
+    }
+}
+
+/* v |grad phi| per cell. */
+void flo_ls_hamiltonian_f64(int64_t nx, int64_t ny, const double* phi, const double* vel,
+                            double h, double* out) {
+  for (int64_t y = 0; y < ny; ++y)
+    for (int64_t x = 0; x < nx; ++x)
+      out[y * nx + x] = hamiltonian(phi, nx, ny, x, y, h, vel[y * nx + x]);
+}
+
+/* The local eikonal solve per cell (neighbours outside the domain +max). */
+void flo_ls_local_solve_f64(int64_t nx, int64_t ny, const double* d, double h, double* out) {
+  for (int64_t y = 0; y < ny; ++y)
+    for (int64_t x = 0; x < nx; ++x) out[y * nx + x] = eik_local(d, nx, ny, x, y, h);
+}
 
 /* Reinitialisation to a signed distance.  Sources are the cells next to a
  * sign change that are nearer the interface than that neighbour

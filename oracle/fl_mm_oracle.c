@@ -18,14 +18,21 @@
  *    wins (a sequential raster loop);
  *  - a source whose level-set gradient vanishes is skipped, and a target
  *    outside the domain is not written;
- *  - the probe states use the bilinear weights the reference documents
- *    (math/interp.hpp:88-104, the 2-D overload at :120-167): x1 = A(1-fx) + B fx, x2 = C(1-fx) + D fx,
- *    r = x1(1-fy) + x2 fy, in double;
+ *  - the probe states use the arithmetic of the reference's 2-D math::interp
+ *    (math/interp.hpp:120-167) as it computes, which is not the bilinear form
+ *    its comment documents: with X0, X1 the cells offset by off_x and
+ *    off_x + sign along x from the source and Y0, Y1 those offset along y,
+ *    close = X0(1-fx) + X1 fx, far = Y0(1-fx) + Y1 fx, r = close(1-fy) + far fy,
+ *    in double (pinned to the reference's function, tests/test_levelset_pinned.py);
  *  - the extrapolation is a Jacobi iteration over the band cells, stopped
  *    when no cell changes by 1e-8 or more (L1 over the components, the
  *    reference's per-cell tolerance) or after max_iters sweeps.
- * Parity pin: none against a run of the reference (its multimaterial driver
- * does not run); the CUDA kernels are checked against this file.
+ * Parity pin: the reference's multimaterial driver does not run, but the
+ * per-source body of RiemannGFM::invoke (steps 1-4: normal, probe
+ * interpolation, rotation, two-material HLLC star state, rotation back) runs
+ * on the host with the reference's own functors (oracle/ref_driver_ls.cpp);
+ * flo_mm_gfm_star is pinned to it bit for bit.  The CUDA kernels are checked
+ * against this file.
  */
 #include <float.h>
 #include <math.h>
@@ -100,7 +107,8 @@ static void load4(const double* u, int64_t pitch, int64_t i, double* o) {
   for (int c = 0; c < 4; ++c) o[c] = u[c * pitch + i];
 }
 
-/* bilinear probe of the state around (x, y) with offsets w (in cells). */
+/* probe of the state around (x, y) with offsets w (in cells), with the
+ * arithmetic of the reference's 2-D math::interp (math/interp.hpp:120-167). */
 static void interp2(const double* u, int64_t pitch, int64_t nx, int64_t ny, int64_t x, int64_t y,
                     const double* w, double* out) {
   int64_t off[2];
@@ -113,16 +121,16 @@ static void interp2(const double* u, int64_t pitch, int64_t nx, int64_t ny, int6
     off[d] = (int64_t)((double)sg[d] * ao);
     f[d] = aw - ao;
   }
-  double A[4], B[4], Cc[4], Dd[4];
-  load4(u, pitch, idx(nx, ny, x + off[0], y + off[1]), A);
-  load4(u, pitch, idx(nx, ny, x + off[0] + sg[0], y + off[1]), B);
-  load4(u, pitch, idx(nx, ny, x + off[0], y + off[1] + sg[1]), Cc);
-  load4(u, pitch, idx(nx, ny, x + off[0] + sg[0], y + off[1] + sg[1]), Dd);
-  const double fx1 = 1.0 - f[0], fy1 = 1.0 - f[1];
+  double X0[4], X1[4], Y0[4], Y1[4];
+  load4(u, pitch, idx(nx, ny, x + off[0], y), X0);
+  load4(u, pitch, idx(nx, ny, x + off[0] + sg[0], y), X1);
+  load4(u, pitch, idx(nx, ny, x, y + off[1]), Y0);
+  load4(u, pitch, idx(nx, ny, x, y + off[1] + sg[1]), Y1);
+  const double factor = 1.0 - f[0];
   for (int c = 0; c < 4; ++c) {
-    const double x1 = A[c] * fx1 + B[c] * f[0];
-    const double x2 = Cc[c] * fx1 + Dd[c] * f[0];
-    out[c] = x1 * fy1 + x2 * f[1];
+    const double close = X0[c] * factor + X1[c] * f[0];
+    const double far = Y0[c] * factor + Y1[c] * f[0];
+    out[c] = close * (1.0 - f[1]) + far * f[1];
   }
 }
 
@@ -175,6 +183,26 @@ static void gfm_star(const double* ua, const double* ub, int64_t pitch, int64_t 
     const double sv = star[2 + d] / star[0];
     const double v = vl[d] + (sv - vl_n) * n[d];
     star[2 + d] = v * star[0];
+  }
+}
+
+/* Star states of listed source cells of material A (the per-source body of
+ * the GFM), with the target offsets sign(n); cells that are not GFM sources
+ * (gfm_source) get NaN and a zero offset. */
+void flo_mm_gfm_star(int64_t nx, int64_t ny, int64_t pitch, double h, const double* ua,
+                     const double* ub, const double* pa, const double* pb, double ga, double ia,
+                     double gb, double ib, int64_t ncells, const int64_t* xs, const int64_t* ys,
+                     double* stars, int* tx, int* ty) {
+  for (int64_t k = 0; k < ncells; ++k) {
+    double n[2];
+    if (!gfm_source(pa, pb, nx, ny, xs[k], ys[k], h, n)) {
+      for (int c = 0; c < 4; ++c) stars[4 * k + c] = NAN;
+      tx[k] = ty[k] = 0;
+      continue;
+    }
+    gfm_star(ua, ub, pitch, nx, ny, pa, xs[k], ys[k], h, n, ga, gb, ia, ib, stars + 4 * k);
+    tx[k] = isgn(n[0]);
+    ty[k] = isgn(n[1]);
   }
 }
 

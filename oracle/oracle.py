@@ -92,6 +92,21 @@ def lib():
         L.flo_ls_velocity_f64.argtypes = [C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_int64, C.c_double, C.c_void_p]
         L.flo_ls_project_f64.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
+        L.flo_ls_weno_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double, C.c_void_p,
+                                      C.c_void_p]
+        L.flo_ls_godunov_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
+                                         C.c_void_p, C.c_void_p]
+        L.flo_ls_hamiltonian_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                             C.c_double, C.c_void_p]
+        L.flo_ls_rk3_stages_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                            C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+        L.flo_ls_local_solve_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
+                                             C.c_void_p]
+        L.flo_mm_gfm_star.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, C.c_int64,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
         L.flo_ls_reinit_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
                                         C.c_void_p, C.c_int]
         L.flo_ls_reinit_f64.restype = C.c_int
@@ -143,6 +158,22 @@ def ref():
         L.ref_star_left_2d.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                        C.c_double, C.c_double, C.c_void_p]
         L.ref_prim_to_cons_f64.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p]
+        L.ref_ls_weno_2d.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double, C.c_void_p,
+                                     C.c_void_p]
+        L.ref_ls_godunov_2d.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
+                                        C.c_void_p, C.c_void_p]
+        L.ref_ls_hamiltonian_2d.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                            C.c_double, C.c_void_p]
+        L.ref_ls_rk3_stage2_2d.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+        L.ref_ls_local_solve_2d.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
+                                            C.c_void_p]
+        L.ref_ls_velocity_2d.argtypes = [C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_int64, C.c_double, C.c_void_p]
+        L.ref_gfm_star_2d.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _ref = L
     return _ref
 
@@ -394,6 +425,100 @@ def ls_velocity(nx, ny, phis, states, h):
     out = np.empty(nx * ny, dtype=np.float64)
     lib().flo_ls_velocity_f64(nx, ny, len(phis), pp, sp, pitch, h, _ptr(out))
     return out
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def ls_weno(nx, ny, phi, h, ref=False):
+    """One-sided WENO-HJ5 derivatives (back, fwrd), each (2, cells): the
+    oracle's, or with ref=True the reference's HJWeno5 functors."""
+    phi = _f64(phi)
+    back = np.empty((2, nx * ny))
+    fwrd = np.empty((2, nx * ny))
+    f = globals()["ref"]().ref_ls_weno_2d if ref else lib().flo_ls_weno_f64
+    f(nx, ny, _ptr(phi), h, _ptr(back), _ptr(fwrd))
+    return back, fwrd
+
+
+def ls_godunov(nx, ny, phi, h, ref=False):
+    """Godunov upwind |grad phi| for v <= 0 (forward) and v > 0 (backward)."""
+    phi = _f64(phi)
+    fwd = np.empty(nx * ny)
+    bwd = np.empty(nx * ny)
+    f = globals()["ref"]().ref_ls_godunov_2d if ref else lib().flo_ls_godunov_f64
+    f(nx, ny, _ptr(phi), h, _ptr(fwd), _ptr(bwd))
+    return fwd, bwd
+
+
+def ls_hamiltonian(nx, ny, phi, vel, h, ref=False):
+    phi, vel = _f64(phi), _f64(vel)
+    out = np.empty(nx * ny)
+    f = globals()["ref"]().ref_ls_hamiltonian_2d if ref else lib().flo_ls_hamiltonian_f64
+    f(nx, ny, _ptr(phi), _ptr(vel), h, _ptr(out))
+    return out
+
+
+def ls_rk3_stages(nx, ny, phi, vel, dt, h):
+    """The oracle's first two RK3 stages (s1, s2)."""
+    phi, vel = _f64(phi), _f64(vel)
+    s1, s2 = np.empty(nx * ny), np.empty(nx * ny)
+    lib().flo_ls_rk3_stages_f64(nx, ny, _ptr(phi), _ptr(vel), dt, h, _ptr(s1), _ptr(s2))
+    return s1, s2
+
+
+def ref_ls_rk3_stage2(nx, ny, phi, stage1, vel, dt, h):
+    """The reference's RungeKutta3::update_impl second stage per cell, given
+    the first stage over the whole grid."""
+    phi, stage1, vel = _f64(phi), _f64(stage1), _f64(vel)
+    out = np.empty(nx * ny)
+    ref().ref_ls_rk3_stage2_2d(nx, ny, _ptr(phi), _ptr(stage1), _ptr(vel), dt, h, _ptr(out))
+    return out
+
+
+def ls_local_solve(nx, ny, d, h, ref=False):
+    d = _f64(d)
+    out = np.empty(nx * ny)
+    f = globals()["ref"]().ref_ls_local_solve_2d if ref else lib().flo_ls_local_solve_f64
+    f(nx, ny, _ptr(d), h, _ptr(out))
+    return out
+
+
+def ref_ls_velocity(nx, ny, phis, states, h):
+    """The reference's per-cell set_velocities body (see ls_velocity)."""
+    phis = [_f64(p) for p in phis]
+    states = [_f64(s) for s in states]
+    pitch = states[0].shape[1]
+    pp = (C.c_void_p * len(phis))(*[p.ctypes.data for p in phis])
+    sp = (C.c_void_p * len(states))(*[s.ctypes.data for s in states])
+    out = np.empty(nx * ny, dtype=np.float64)
+    ref().ref_ls_velocity_2d(nx, ny, len(phis), pp, sp, pitch, h, _ptr(out))
+    return out
+
+
+def gfm_star(nx, ny, h, ua, ub, pa, pb, gammas, p_infs, xs, ys, ref=False):
+    """Star states (4, k) and target offsets (tx, ty) of the GFM for source
+    cells (xs, ys) of material A: the oracle's (cells that are not sources
+    get NaN), or with ref=True the reference's per-source body."""
+    ua, ub, pa = _f64(ua), _f64(ub), _f64(pa)
+    pitch = ua.shape[1]
+    xs = np.ascontiguousarray(xs, dtype=np.int64)
+    ys = np.ascontiguousarray(ys, dtype=np.int64)
+    k = xs.size
+    stars = np.empty((k, 4))
+    tx = np.zeros(k, dtype=np.int32)
+    ty = np.zeros(k, dtype=np.int32)
+    (ga, gb), (ia, ib) = gammas, p_infs
+    if ref:
+        globals()["ref"]().ref_gfm_star_2d(nx, ny, pitch, h, _ptr(ua), _ptr(ub), _ptr(pa), ga, ia,
+                                           gb, ib, k, _ptr(xs), _ptr(ys), _ptr(stars), _ptr(tx),
+                                           _ptr(ty))
+    else:
+        pb = _f64(pb)
+        lib().flo_mm_gfm_star(nx, ny, pitch, h, _ptr(ua), _ptr(ub), _ptr(pa), _ptr(pb), ga, ia,
+                              gb, ib, k, _ptr(xs), _ptr(ys), _ptr(stars), _ptr(tx), _ptr(ty))
+    return stars.T.copy(), tx, ty
 
 
 def ls_project(a, b):

@@ -350,3 +350,8 @@ int64_t ref_simulate_f64(int dims, const int64_t* n, int64_t pitch, double* a,
 }
 
 }  // extern "C"
+
+// The level-set functors' driver.  The reference's headers define some
+// functions outside classes without `inline` (state/state_components.hpp's
+// literal operators), so the whole driver is one translation unit.
+#include "ref_driver_ls.cpp"

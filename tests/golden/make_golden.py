@@ -8,9 +8,15 @@ oracle/_ref/libfluidity_ref.so and driven by oracle/ref_driver.cpp.  Inputs
 are seeded.  Run from the repository root (needs the reference tree to build
 the library):
 
-    bash oracle/build_ref.sh && python tests/golden/make_golden.py
+    bash oracle/build_ref.sh REFERENCE_ROOT && python tests/golden/make_golden.py
 
 stiff.npz holds the same kinds of cases for the stiffened fluid.
+
+levelset.npz holds the reference's level-set functors on seeded 2-D fields
+(oracle/ref_driver_ls.cpp): HJWeno5 one-sided derivatives, GodunovUpwind
+gradients, LevelsetHamiltonian values, the first two RungeKutta3 stages, the
+GodunovUpwindScheme local eikonal solve and the set_velocities cell body.
+`python tests/golden/make_golden.py levelset` regenerates that file alone.
 """
 import os
 import sys
@@ -161,6 +167,82 @@ def stiff_cases():
     return cases
 
 
+def levelset_cases():
+    cases = {}
+    rng = np.random.default_rng(2024)
+    big = np.finfo(np.float64).max
+
+    def grid(nx, ny):
+        h = 1.0 / ny
+        x = (np.arange(nx) + 0.5) * h
+        y = (np.arange(ny) + 0.5) * h
+        return h, np.meshgrid(x, y)
+
+    specs = []
+    h, (X, Y) = grid(40, 32)
+    specs.append(("circle_40x32", 40, 32, h, np.sqrt((X - 0.6) ** 2 + (Y - 0.5) ** 2) - 0.3,
+                  np.sin(3 * X) * np.cos(2 * Y)))
+    h, (X, Y) = grid(36, 28)
+    d1 = np.sqrt((X - 0.4) ** 2 + (Y - 0.5) ** 2) - 0.25
+    d2 = np.sqrt((X - 0.9) ** 2 + (Y - 0.45) ** 2) - 0.2
+    specs.append(("two_circles_36x28", 36, 28, h, np.minimum(d1, d2), -0.5 + X - 0.3 * Y))
+    h, (X, Y) = grid(24, 20)
+    specs.append(("wavy_24x20", 24, 20, h,
+                  0.3 * np.sin(2 * np.pi * X) + 0.2 * np.cos(3 * np.pi * Y) - 0.1,
+                  rng.uniform(-1.0, 1.0, (20, 24))))
+    h, (X, Y) = grid(4, 40)
+    specs.append(("thin_4x40", 4, 40, h, np.sin(5 * Y) - 0.3 + 0.1 * X,
+                  rng.uniform(-2.0, 2.0, (40, 4))))
+    for name, nx, ny, h, phi, vel in specs:
+        phi = np.ascontiguousarray(phi.ravel())
+        vel = np.ascontiguousarray(vel.ravel())
+        back, fwrd = O.ls_weno(nx, ny, phi, h, ref=True)
+        gf, gb = O.ls_godunov(nx, ny, phi, h, ref=True)
+        ham = O.ls_hamiltonian(nx, ny, phi, vel, h, ref=True)
+        dt = 0.4 * h / np.max(np.abs(vel))
+        stage1 = phi - dt * ham                # RungeKutta3::update_impl's first line
+        stage2 = O.ref_ls_rk3_stage2(nx, ny, phi, stage1, vel, dt, h)
+        # local eikonal solve: a band of distances near the interface (a
+        # fast-iterative-method start) and, separately, distances with noise
+        band = np.where(np.abs(phi) < 1.5 * h, np.abs(phi), big)
+        noisy = np.abs(phi) * (1.0 + 0.05 * rng.standard_normal(phi.size))
+        loc_band = O.ls_local_solve(nx, ny, band, h, ref=True)
+        loc_noisy = O.ls_local_solve(nx, ny, noisy, h, ref=True)
+        states = [np.vstack([rng.uniform(0.5, 2.0, phi.size), rng.uniform(2.0, 8.0, phi.size),
+                             rng.uniform(-1.0, 1.0, phi.size), rng.uniform(-1.0, 1.0, phi.size)])
+                  for _ in range(2)]
+        v = O.ref_ls_velocity(nx, ny, [phi, -phi], states, h)
+        cases[name] = dict(nx=nx, ny=ny, h=h, dt=dt, phi=phi, vel=vel, back=back, fwrd=fwrd,
+                           god_fwd=gf, god_bwd=gb, ham=ham, stage1=stage1, stage2=stage2,
+                           band=band, local_band=loc_band, noisy=noisy, local_noisy=loc_noisy,
+                           state0=states[0], state1=states[1], velocity=v)
+    # Riemann ghost fluid: star states and targets of every source cell of a
+    # circular interface, for ideal-gas and stiffened-fluid pairings
+    h, (X, Y) = grid(48, 40)
+    pa = (np.sqrt((X - 0.6) ** 2 + (Y - 0.5) ** 2) - 0.3).ravel()
+
+    def smooth_states(g, pinf, k):
+        rho = 1.0 + 0.3 * np.sin((5 + k) * X) * np.cos(3 * Y)
+        u = 0.3 * np.cos((4 + k) * Y)
+        v = 0.2 * np.sin(3 * X + k)
+        p = 1.0 + 0.5 * np.cos(2 * X + Y)
+        e = (p + g * pinf) / (g - 1.0) + 0.5 * rho * (u * u + v * v)
+        return np.vstack([rho.ravel(), e.ravel(), (rho * u).ravel(), (rho * v).ravel()])
+
+    cand = np.nonzero((pa <= 0.0) & (pa >= -h))[0]
+    for k, ((ga, gb), (ia, ib)) in enumerate([((1.4, 1.67), (0.0, 0.0)),
+                                               ((1.4, 4.4), (0.0, 0.6)),
+                                               ((5.5, 1.4), (0.613, 0.0)),
+                                               ((4.4, 5.5), (0.3, 0.613))]):
+        ua, ub = smooth_states(ga, ia, k), smooth_states(gb, ib, k + 1)
+        xs, ys = cand % 48, cand // 48
+        stars, tx, ty = O.gfm_star(48, 40, h, ua, ub, pa, -pa, (ga, gb), (ia, ib), xs, ys,
+                                   ref=True)
+        cases[f"gfm_{k}"] = dict(nx=48, ny=40, h=h, ua=ua, ub=ub, pa=pa, ga=ga, gb=gb, ia=ia,
+                                 ib=ib, xs=xs, ys=ys, stars=stars, tx=tx, ty=ty)
+    return cases
+
+
 def check_finite(cases):
     # multi-step cases must stay finite: a blown-up state (NaN) is flagged as
     # an error by the GPU path, while the reference's max_element silently
@@ -191,6 +273,11 @@ def load(name):
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("oracle/_ref/libfluidity_ref.so missing: run oracle/build_ref.sh first")
+    if sys.argv[1:] == ["levelset"]:
+        save("levelset.npz", levelset_cases())
+        print("levelset.npz", os.path.getsize(os.path.join(OUT, "levelset.npz")), "bytes")
+        sys.exit(0)
+    save("levelset.npz", levelset_cases())
     save("sweeps.npz", sweep_cases())
     sims = simulate_cases()
     check_finite(sims)
@@ -198,5 +285,5 @@ if __name__ == "__main__":
     stiff = stiff_cases()
     check_finite({k: v for k, v in stiff.items() if "out" in v and "dim" not in v})
     save("stiff.npz", stiff)
-    for f in ("sweeps.npz", "simulate.npz", "stiff.npz"):
+    for f in ("sweeps.npz", "simulate.npz", "stiff.npz", "levelset.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
