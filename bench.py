@@ -371,6 +371,7 @@ def run_ours(a, world, rank, local):
         e2e_value = world * cells * T * e2e_steps / e2e_s
         del pipe
 
+    drop_in = measure_drop_in(a, s, states, sweep_s)
     variants = {}
     ref_cache = {}
     headline_checks = None
@@ -412,6 +413,7 @@ def run_ours(a, world, rank, local):
         "gpu_launches": a.steps * (3 + launches_per_run + alternating_transposes(a)),
         "clocks": clocks,
     }
+    line["drop_in"] = drop_in
     if headline_checks is not None:
         line.update(headline_checks)
     if variants:
@@ -430,6 +432,32 @@ def run_ours(a, world, rank, local):
     if rank == 0:
         print(json.dumps(line))
     del sim
+
+
+def measure_drop_in(a, s, states, loop_sweep_s, steps=20):
+    """The drop-in step on the headline grid: fl_split_solve_ws (the
+    reference's SplitSolver::solve interface with a caller-owned workspace)
+    for `steps` steps at the initial CFL time step, timed with CUDA events;
+    per-sweep time against the device-resident loop's."""
+    import torch
+    x, y = s.new_state(), s.new_state()
+    s.fill_riemann(states, out=x)
+    dtdh = 0.8 / s.max_wavespeed(x).item()
+    mws = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(2):                                   # warm-up
+        x, y = s.solve(x, y, dtdh, max_ws=mws)[::-1]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        x, y = s.solve(x, y, dtdh, max_ws=mws)[::-1]
+    e1.record()
+    torch.cuda.synchronize()
+    sweep_ms = e0.elapsed_time(e1) / (steps * len(s.shape))
+    del x, y
+    torch.cuda.empty_cache()
+    return {"api": "fl_split_solve_ws (caller-owned workspace, strips taken dynamically)",
+            "steps": steps, "sweep_ms": sweep_ms, "loop_sweep_ms": loop_sweep_s * 1e3,
+            "ratio_to_loop": sweep_ms / (loop_sweep_s * 1e3)}
 
 
 def measure_variant(a, dtype, flux, states, runs=3):

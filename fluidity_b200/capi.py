@@ -92,6 +92,12 @@ PROTOTYPES = {
     "fl_split_solve_mat": (C.c_int, [_G, C.POINTER(_P), C.POINTER(_P), C.POINTER(Material),
                                      C.c_double, C.c_uint32, C.c_uint32, _P, _P]),
     "fl_max_wavespeed_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
+    "fl_workspace_bytes": (C.c_int64, [_G, C.c_uint32]),
+    "fl_split_sweep_ws": (C.c_int, [_G, C.c_int, _P, _P, C.POINTER(Material), C.c_double,
+                                    C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "fl_split_solve_ws": (C.c_int, [_G, C.POINTER(_P), C.POINTER(_P), C.POINTER(Material),
+                                    C.c_double, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "fl_workspace_status": (C.c_int, [_P, _P, C.POINTER(C.c_int)]),
     "fl_fill_riemann_mat": (C.c_int, [_G, _P, C.POINTER(Material), C.c_uint32, _P, _P]),
     "fl_sim_set_material": (C.c_int, [_P, C.POINTER(Material)]),
     "fl_host_pipe_create": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,

@@ -373,7 +373,17 @@ namespace fl {
 int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
                         const fl_material* mat, double dtdh, uint32_t policy,
                         uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
-                        int walk_slot, void* stream);
+                        int walk_slot, void* stream, void* scratch = nullptr,
+                        int* status = nullptr);
+
+// Workspace of the drop-in sweep (fl_workspace_bytes): two strip counters and
+// a status word in the first 256 bytes, then, for 3-D grids, the register
+// walk's chi plane (one value per cell).
+constexpr size_t kWsHead = 256;
+struct WorkspaceHead {
+  unsigned int walk_next[2];
+  int status;
+};
 }  // namespace fl
 
 extern "C" {
@@ -389,12 +399,14 @@ int fl_split_sweep_mat(const fl_grid* grid, int dim, const void* in, void* out,
 
 namespace fl {
 
-// fl_split_sweep_mat with strip counters (nullable) and their parity slot;
-// the two-material loop owns a pair.
+// fl_split_sweep_mat with strip counters (nullable) and their parity slot
+// (the two-material loop owns a pair), the 3-D walk's chi plane (nullable:
+// without it 3-D sweeps take the tile kernel) and a status word (nullable).
+// Allocates nothing.
 int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
                         const fl_material* mat, double dtdh, uint32_t policy,
                         uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
-                        int walk_slot, void* stream) {
+                        int walk_slot, void* stream, void* scratch, int* status) {
   int rc = check_grid(grid);
   if (rc) return rc;
   if ((rc = check_policy(policy))) return rc;
@@ -415,21 +427,31 @@ int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
     if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
     p.ws_accum = reinterpret_cast<unsigned long long*>(max_ws_out);
   }
-  // 3-D: the walk's chi plane, from the stream-ordered pool for this call
-  void* scratch = nullptr;
-  if (grid->dims == 3) {
-    const size_t bytes = (size_t)(grid->n[0] * grid->n[1] * grid->n[2]) * elem_size(pol);
-    cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
-    if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep: scratch");
-    p.scratch = scratch;
-  }
+  p.scratch = (grid->dims == 3) ? scratch : nullptr;
+  p.status = status;
   cudaError_t e = launch_sweep(p, pol, grid->dims, dim, st);
-  if (scratch != nullptr) {
-    const cudaError_t f = cudaFreeAsync(scratch, st);
-    if (e == cudaSuccess) e = f;
-  }
   if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep");
   return kOk;
+}
+
+// The drop-in sweep with a caller's workspace: the counter it takes strips
+// from is cleared on the stream first, so that calls need no parity of
+// their own.
+int split_sweep_ws(const fl_grid* grid, int dim, const void* in, void* out,
+                   const fl_material* mat, double dtdh, uint32_t policy, uint32_t boundary_mask,
+                   double* max_ws_out, void* workspace, void* stream) {
+  if (workspace == nullptr) return fail(kEInval, "workspace is NULL");
+  if (reinterpret_cast<uintptr_t>(workspace) & 255u)
+    return fail(kEInval, "workspace must be 256-byte aligned");
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  auto* head = static_cast<WorkspaceHead*>(workspace);
+  cudaError_t e = cudaMemsetAsync(&head->walk_next[0], 0, sizeof(unsigned int),
+                                  static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "fl_split_sweep_ws");
+  void* plane = (grid->dims == 3) ? static_cast<char*>(workspace) + kWsHead : nullptr;
+  return split_sweep_counted(grid, dim, in, out, mat, dtdh, policy, boundary_mask, max_ws_out,
+                             head->walk_next, 0, stream, plane, &head->status);
 }
 
 }  // namespace fl
@@ -468,6 +490,55 @@ int fl_split_solve(const fl_grid* grid, void** in, void** out, double gamma, dou
                    uint32_t policy, uint32_t boundary_mask, double* max_ws_out, void* stream) {
   const fl_material mat{gamma, 0.0};
   return fl_split_solve_mat(grid, in, out, &mat, dtdh, policy, boundary_mask, max_ws_out, stream);
+}
+
+int64_t fl_workspace_bytes(const fl_grid* grid, uint32_t policy) {
+  if (check_grid(grid) != kOk || check_policy(policy) != kOk) return -1;
+  int64_t bytes = (int64_t)kWsHead;
+  if (grid->dims == 3)
+    bytes += (grid->n[0] * grid->n[1] * grid->n[2] * (int64_t)elem_size(decode(policy)) + 255) /
+             256 * 256;
+  return bytes;
+}
+
+int fl_split_sweep_ws(const fl_grid* grid, int dim, const void* in, void* out,
+                      const fl_material* mat, double dtdh, uint32_t policy,
+                      uint32_t boundary_mask, double* max_ws_out, void* workspace,
+                      void* stream) {
+  return fl::split_sweep_ws(grid, dim, in, out, mat, dtdh, policy, boundary_mask, max_ws_out,
+                            workspace, stream);
+}
+
+int fl_split_solve_ws(const fl_grid* grid, void** in, void** out, const fl_material* mat,
+                      double dtdh, uint32_t policy, uint32_t boundary_mask, double* max_ws_out,
+                      void* workspace, void* stream) {
+  if (in == nullptr || out == nullptr) return fail(kEInval, "NULL buffer handle");
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  for (int d = 0; d < grid->dims; ++d) {
+    double* ws = (d == grid->dims - 1) ? max_ws_out : nullptr;
+    rc = fl::split_sweep_ws(grid, d, *in, *out, mat, dtdh, policy, boundary_mask, ws, workspace,
+                            stream);
+    if (rc) return rc;
+    if (grid->dims != 1 && d < grid->dims - 1) {
+      void* t = *in;
+      *in = *out;
+      *out = t;
+    }
+  }
+  return kOk;
+}
+
+int fl_workspace_status(const void* workspace, void* stream, int* status) {
+  if (workspace == nullptr || status == nullptr) return fail(kEInval, "NULL argument");
+  int h = 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(&h, &static_cast<const WorkspaceHead*>(workspace)->status,
+                                  sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "fl_workspace_status");
+  *status = h;
+  return kOk;
 }
 
 int fl_max_wavespeed_mat(const fl_grid* grid, const void* in, const fl_material* mat,

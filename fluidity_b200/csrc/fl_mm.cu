@@ -36,7 +36,8 @@ namespace fl {
 int split_sweep_counted(const fl_grid* grid, int dim, const void* in, void* out,
                         const fl_material* mat, double dtdh, uint32_t policy,
                         uint32_t boundary_mask, double* max_ws_out, unsigned int* walk_next,
-                        int walk_slot, void* stream);
+                        int walk_slot, void* stream, void* scratch = nullptr,
+                        int* status = nullptr);
 
 namespace {
 

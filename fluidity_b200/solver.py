@@ -44,12 +44,17 @@ class SplitSolver:
 
     p_inf = 0 is the ideal gas (material/ideal_gas.hpp); p_inf > 0 the
     stiffened fluid StiffFluid(gamma, p_inf) (material/stiff_fluid.hpp:38-133),
-    through the C ABI's fl_material entry points."""
+    through the C ABI's fl_material entry points.
+
+    workspace=True (the default) sweeps through fl_split_sweep_ws /
+    fl_split_solve_ws with a workspace allocated once here: strips taken
+    dynamically and, in 3-D, the register walk.  workspace=False takes the
+    plain entry points (one strip per warp; 3-D through the tile kernel)."""
 
     def __init__(self, shape, dtype: str = "f64", flux: str = "hllc",
                  limiter: str = "vanleer", recon: str = "muscl", gamma: float = 1.4,
                  boundary_mask: int = 0, flatten: bool = True, pitch: int | None = None,
-                 p_inf: float = 0.0):
+                 p_inf: float = 0.0, workspace: bool = True):
         self.shape = tuple(int(v) for v in shape)
         self.dims = len(self.shape)
         self.dtype = dtype
@@ -60,6 +65,22 @@ class SplitSolver:
         self.policy = capi.policy_bits(dtype, flux, limiter, recon, flatten)
         self.grid = capi.Grid.make(self.shape, pitch)
         self.lib = capi.load()
+        self.workspace = None
+        if workspace:
+            nbytes = self.lib.fl_workspace_bytes(C.byref(self.grid), self.policy)
+            if nbytes < 0:
+                capi.check(capi.FL_EINVAL, self.lib)
+            self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+
+    def _ws(self):
+        return C.c_void_p(self.workspace.data_ptr())
+
+    def workspace_status(self, stream=None) -> int:
+        """The workspace's status word (0, or FL_ETIMEOUT); synchronises."""
+        st = C.c_int()
+        capi.check(self.lib.fl_workspace_status(self._ws(), _stream_ptr(stream), C.byref(st)),
+                   self.lib)
+        return st.value
 
     def new_state(self):
         return state_tensor(self.shape, self.dtype, pitch=self.grid.pitch)
@@ -69,7 +90,11 @@ class SplitSolver:
         the max wavespeed of dst."""
         ws = None if max_ws is None else C.c_void_p(max_ws.data_ptr())
         args = (C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()))
-        if self.p_inf != 0.0:
+        if self.workspace is not None:
+            rc = self.lib.fl_split_sweep_ws(C.byref(self.grid), int(dim), *args,
+                                            C.byref(self.material), float(dtdh), self.policy,
+                                            self.boundary_mask, ws, self._ws(), _stream_ptr(stream))
+        elif self.p_inf != 0.0:
             rc = self.lib.fl_split_sweep_mat(C.byref(self.grid), int(dim), *args,
                                              C.byref(self.material), float(dtdh), self.policy,
                                              self.boundary_mask, ws, _stream_ptr(stream))
@@ -84,7 +109,11 @@ class SplitSolver:
         pin = C.c_void_p(src.data_ptr())
         pout = C.c_void_p(dst.data_ptr())
         ws = None if max_ws is None else C.c_void_p(max_ws.data_ptr())
-        if self.p_inf != 0.0:
+        if self.workspace is not None:
+            rc = self.lib.fl_split_solve_ws(C.byref(self.grid), C.byref(pin), C.byref(pout),
+                                            C.byref(self.material), float(dtdh), self.policy,
+                                            self.boundary_mask, ws, self._ws(), _stream_ptr(stream))
+        elif self.p_inf != 0.0:
             rc = self.lib.fl_split_solve_mat(C.byref(self.grid), C.byref(pin), C.byref(pout),
                                              C.byref(self.material), float(dtdh), self.policy,
                                              self.boundary_mask, ws, _stream_ptr(stream))

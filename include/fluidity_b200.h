@@ -96,10 +96,10 @@ int64_t fl_state_bytes(const fl_grid* grid, uint32_t policy);
  * max_d |u_d| + a of the OUTPUT state -- the fused form of set_wavespeeds +
  * max_element (simulator/cuda/wavespeed_initialization.cuh:85-97,
  * algorithm/max_element.hpp:28-38) for the next step.
- * 3-D grids take one cell-count plane of scratch from the device's
- * stream-ordered pool (cudaMallocAsync on `stream`) for the call; fl_sim_*
- * allocate theirs once at fl_sim_create, and fl_simulate_noalloc uses none
- * (its 3-D sweeps take the shared-memory tile kernel). */
+ * Allocates nothing.  Strips are scheduled one per warp; 3-D sweeps take the
+ * shared-memory tile kernel.  fl_split_sweep_ws (below) takes a workspace
+ * and with it schedules strips dynamically and sweeps 3-D grids with the
+ * register walk. */
 int fl_split_sweep(const fl_grid* grid, int dim, const void* in, void* out,
                    double gamma, double dtdh, uint32_t policy,
                    uint32_t boundary_mask, double* max_ws_out, void* stream);
@@ -158,6 +158,32 @@ int fl_max_wavespeed_mat(const fl_grid* grid, const void* in, const fl_material*
 int fl_fill_riemann_mat(const fl_grid* grid, const double* states_prim,
                         const fl_material* mat, uint32_t policy, void* out,
                         void* stream);
+
+/* ---- the drop-in step with a workspace --------------------------------
+ * Replaces SplitSolver::solve / solve_impl_split (solver/split_solver.hpp
+ * :105-115, solver/cuda/split_solver.cuh:57-80) and solve_dim /
+ * SplitSolver::invoke (split_solver.cuh:39-44, split_solver.hpp:138-162) as
+ * fl_split_sweep / fl_split_solve do, with a caller-owned workspace of
+ * fl_workspace_bytes(grid, policy) bytes of device memory, 256-byte aligned:
+ * two strip counters and a status word, and for 3-D grids one value per
+ * cell of scratch for the register walk's flattening plane.  The calls
+ * allocate nothing; the workspace needs no initialisation (each sweep
+ * clears the counter it uses on `stream`).  Strips are taken dynamically
+ * by the CTAs resident on the GPU, as in the device-resident loop.  Sweeps
+ * sharing one workspace must be ordered on one stream.  A sweep whose
+ * bounded wait for its staged copies gave up leaves FL_ETIMEOUT in the
+ * status word (fl_workspace_status); it is never set otherwise. */
+int64_t fl_workspace_bytes(const fl_grid* grid, uint32_t policy);
+int fl_split_sweep_ws(const fl_grid* grid, int dim, const void* in, void* out,
+                      const fl_material* mat, double dtdh, uint32_t policy,
+                      uint32_t boundary_mask, double* max_ws_out, void* workspace,
+                      void* stream);
+int fl_split_solve_ws(const fl_grid* grid, void** in, void** out, const fl_material* mat,
+                      double dtdh, uint32_t policy, uint32_t boundary_mask,
+                      double* max_ws_out, void* workspace, void* stream);
+/* Reads the workspace's status word after `stream` has finished (it
+ * synchronises the stream): 0, or FL_ETIMEOUT. */
+int fl_workspace_status(const void* workspace, void* stream, int* status);
 
 /* Layout adapters for the reference's AoS DeviceTensor<State, D>
  * (container/device_tensor.hpp): aos holds cells * (dims + 2) values. */

@@ -20,6 +20,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <memory>
 #include <vector>
 
 #include "../fluidity_b200.h"
@@ -254,7 +255,11 @@ struct SplitSolver {
 
   // solve(in, out, mat, dtdh, setter): all sweeps, x -> y -> z, swapping in
   // and out between sweeps like split_solver.cuh:67-79; afterwards `out`
-  // refers to the new state.  stream defaults to the legacy stream.
+  // refers to the new state.  stream defaults to the legacy stream.  The
+  // step itself allocates nothing: the solver keeps one workspace
+  // (fl_workspace_bytes; strip counters, and in 3-D the flattening plane),
+  // allocated on the first solve for that grid and shared by copies of the
+  // solver; solves sharing it must be ordered on one stream.
   template <typename Mat>
   void solve(DeviceStates<value_t, num_dimensions>& in,
              DeviceStates<value_t, num_dimensions>& out, const Mat& mat, value_t dtdh,
@@ -263,10 +268,25 @@ struct SplitSolver {
     void* pin = in.data();
     void* pout = out.data();
     const fl_material m = material::to_fl(mat);
-    check(fl_split_solve_mat(&in.grid(), &pin, &pout, &m, (double)dtdh, policy, setter.mask,
-                             max_ws_out, stream));
+    check(fl_split_solve_ws(&in.grid(), &pin, &pout, &m, (double)dtdh, policy, setter.mask,
+                            max_ws_out, workspace(in.grid()), stream));
     if (pout != out.data()) in.swap(out);
   }
+
+ private:
+  void* workspace(const fl_grid& g) const {
+    const int64_t bytes = fl_workspace_bytes(&g, policy);
+    if (bytes < 0) throw std::runtime_error(fl_last_error_string());
+    if (!ws_ || ws_bytes_ < bytes) {
+      void* p = nullptr;
+      check_cuda(cudaMalloc(&p, (std::size_t)bytes));
+      ws_ = std::shared_ptr<void>(p, [](void* q) { cudaFree(q); });
+      ws_bytes_ = bytes;
+    }
+    return ws_.get();
+  }
+  mutable std::shared_ptr<void> ws_;
+  mutable int64_t ws_bytes_ = 0;
 };
 
 }  // namespace solver

@@ -485,21 +485,26 @@ def test_f32_l1_against_f64_oracle(cuda, oracle, seed):
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 @pytest.mark.parametrize("shape", [(2048, 2048), (1024, 1024), (700, 300)])
 def test_dynamic_strips_equal_static_grid(cuda, dtype, shape):
-    """The device-resident loop takes its strips dynamically (64-row strips
-    at 2048^2, shortened to 32 rows where 64-row strips cannot fill the
-    GPU); fl_split_solve launches the static grid.  Two steps of each, with
-    the loop's own time steps replayed on the static path.  With the
-    register walk for both (FLUIDITY_B200_SWEEP=walk) they agree bit for
-    bit in FP64: the schedule decides only which warp computes a cell; the
-    walk's two schedules are separately inlined copies of the strip code,
-    which the compiler contracts differently in FP32 (6e-7 relative
-    measured).  By default the FP64 loop alternates layouts and sweeps x
-    with the staged walk while fl_split_solve sweeps x with the register
-    walk: there the two agree to the FP64 parity bar."""
+    """Three paths over two steps, the static ones replaying the loop's own
+    time steps: the device-resident loop (strips taken dynamically; 64-row
+    strips at 2048^2, shortened to 32 rows where 64-row strips cannot fill
+    the GPU), fl_split_solve_ws (the drop-in step with a workspace, strips
+    taken dynamically too) and fl_split_solve (one strip per warp).
+    * fl_split_solve_ws against fl_split_solve: the schedule decides only
+      which warp computes a cell, so FP64 agrees bit for bit.  The register
+      walk's two schedules are separately inlined copies of the strip code,
+      which the compiler contracts differently in FP32 (6e-7 relative
+      measured), so FP32 agrees to rounding.
+    * the loop against fl_split_solve_ws: with the register walk for both
+      (FLUIDITY_B200_SWEEP=walk) bit for bit; by default the FP64 loop
+      alternates layouts and sweeps x with the staged walk while the drop-in
+      step sweeps x with the register walk, and the two agree to the FP64
+      parity bar."""
     import torch
     from fluidity_b200.solver import Simulation, SplitSolver
     from fluidity_b200.workloads import riemann_states
     s = SplitSolver(shape, dtype=dtype, gamma=GAMMA)
+    s_static = SplitSolver(shape, dtype=dtype, gamma=GAMMA, workspace=False)
     a = s.new_state()
     s.fill_riemann(riemann_states(7, 2), out=a)
     u0 = a.clone()
@@ -510,25 +515,83 @@ def test_dynamic_strips_equal_static_grid(cuda, dtype, shape):
     sim.steps(2)
     it, _, done, out = sim.status()
     assert it == 2 and done
-    x, y = u0.clone(), torch.empty_like(u0)
-    ws = s.max_wavespeed(x).item()
-    for _ in range(2):
-        # the time step as the device computes it (finalize_control)
-        if dtype == "f32":
-            f32, f64 = np.float32, np.float64
-            dt = f32(f64(f32(0.8)) * res / f64(f32(ws)))
-            dtdh = float(f32(f64(dt) / res))
-        else:
-            dtdh = (0.8 * res / ws) / res
-        mws = torch.zeros(1, dtype=torch.float64, device="cuda")
-        _, x = s.solve(x, y, dtdh, max_ws=mws)      # 2-D: the result returns to x
-        ws = mws.item()
-    torch.cuda.synchronize()
-    if dtype == "f64" and os.environ.get("FLUIDITY_B200_SWEEP") == "walk":
-        assert torch.equal(out, x)
-    elif dtype == "f64":
-        assert rel_err(out.cpu().numpy(), x.cpu().numpy()) < TOL["f64"]
+    outs = []
+    for solver in (s, s_static):
+        x, y = u0.clone(), torch.empty_like(u0)
+        ws = solver.max_wavespeed(x).item()
+        for _ in range(2):
+            # the time step as the device computes it (finalize_control)
+            if dtype == "f32":
+                f32, f64 = np.float32, np.float64
+                dt = f32(f64(f32(0.8)) * res / f64(f32(ws)))
+                dtdh = float(f32(f64(dt) / res))
+            else:
+                dtdh = (0.8 * res / ws) / res
+            mws = torch.zeros(1, dtype=torch.float64, device="cuda")
+            _, x = solver.solve(x, y, dtdh, max_ws=mws)      # 2-D: the result returns to x
+            ws = mws.item()
+        torch.cuda.synchronize()
+        outs.append(x)
+    dyn, static = outs
+
+    def close(p, q, bar=1e-5):
+        d = (p.double() - q.double()).abs()
+        return (d / q.double().abs().clamp_min(1.0)).max().item() < bar
+
+    if dtype == "f64":
+        assert torch.equal(dyn, static)
     else:
-        d = (out.double() - x.double()).abs()
-        worst = (d / x.double().abs().clamp_min(1.0)).max().item()
-        assert worst < 1e-5, worst
+        assert close(dyn, static)
+    if os.environ.get("FLUIDITY_B200_SWEEP") == "walk":
+        assert torch.equal(out, dyn)
+    elif dtype == "f64":
+        assert rel_err(out.cpu().numpy(), dyn.cpu().numpy()) < TOL["f64"]
+    else:
+        assert close(out, dyn)
+
+
+def test_workspace_bytes_and_checks(cuda):
+    """fl_workspace_bytes: a 256-byte head, plus one value per cell in 3-D;
+    a workspace that is not 256-byte aligned is refused before any launch."""
+    import ctypes as C
+    import torch
+    from fluidity_b200 import capi
+    from fluidity_b200.solver import SplitSolver
+    lib = capi.load()
+    for shape, dtype, want in [((64, 48), "f64", 256), ((10, 8, 6), "f64", 256 + 3840),
+                               ((10, 8, 6), "f32", 256 + 2048), ((400,), "f32", 256)]:
+        s = SplitSolver(shape, dtype=dtype, gamma=GAMMA)
+        assert lib.fl_workspace_bytes(C.byref(s.grid), s.policy) == want
+    s = SplitSolver((64, 48), gamma=GAMMA)
+    a = s.fill_riemann(np.array([[1.0, 1.0, 0.0, 0.0], [0.5, 0.4, 0.1, 0.0],
+                                 [0.8, 0.6, 0.0, 0.1], [0.3, 0.3, 0.0, 0.0]]))
+    b = torch.empty_like(a)
+    raw = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    rc = lib.fl_split_sweep_ws(C.byref(s.grid), 0, C.c_void_p(a.data_ptr()),
+                               C.c_void_p(b.data_ptr()), C.byref(s.material), 0.001, s.policy, 0,
+                               None, C.c_void_p(raw.data_ptr() + 8), None)
+    assert rc == capi.FL_EINVAL
+    assert s.workspace_status() == 0
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_workspace_3d_walk_and_tile_match_oracle(cuda, oracle, dtype):
+    """3-D sweeps: with a workspace the register walk (its flattening plane
+    in the workspace), without one the tile kernel; both at the parity bars,
+    and the workspace reused across calls without being cleared."""
+    import torch
+    from fluidity_b200.solver import SplitSolver
+    shape = (20, 13, 11)
+    npdt = NPDT[dtype]
+    u = oracle.prim_to_cons(random_prim(shape, 3, smooth=True, mild=True), GAMMA, dtype=npdt)
+    ws = float(oracle.max_wavespeed(shape, u, npdt(GAMMA)))
+    dtdh = npdt(0.5 / ws)
+    for workspace in (True, False):
+        s = SplitSolver(shape, dtype=dtype, gamma=GAMMA, workspace=workspace)
+        for dim in (0, 1, 2, 0):
+            ref = oracle.sweep(shape, dim, u, npdt(GAMMA), dtdh)
+            a = to_dev(u, dtype)
+            b = torch.empty_like(a)
+            s.sweep(a, b, dim, float(dtdh))
+            torch.cuda.synchronize()
+            assert err(b.cpu().numpy(), ref, dtype) < TOL[dtype], (workspace, dim)
