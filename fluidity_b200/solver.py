@@ -70,7 +70,7 @@ class SplitSolver:
             nbytes = self.lib.fl_workspace_bytes(C.byref(self.grid), self.policy)
             if nbytes < 0:
                 capi.check(capi.FL_EINVAL, self.lib)
-            self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+            self.workspace = torch.zeros(int(nbytes), dtype=torch.uint8, device="cuda")
 
     def _ws(self):
         return C.c_void_p(self.workspace.data_ptr())

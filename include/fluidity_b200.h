@@ -167,8 +167,9 @@ int fl_fill_riemann_mat(const fl_grid* grid, const double* states_prim,
  * fl_workspace_bytes(grid, policy) bytes of device memory, 256-byte aligned:
  * two strip counters and a status word, and for 3-D grids one value per
  * cell of scratch for the register walk's flattening plane.  The calls
- * allocate nothing; the workspace needs no initialisation (each sweep
- * clears the counter it uses on `stream`).  Strips are taken dynamically
+ * allocate nothing.  Zero the workspace once before its first use (the
+ * status word starts at 0); each sweep clears the strip counter it uses on
+ * `stream`, so nothing needs clearing between calls.  Strips are taken dynamically
  * by the CTAs resident on the GPU, as in the device-resident loop.  Sweeps
  * sharing one workspace must be ordered on one stream.  A sweep whose
  * bounded wait for its staged copies gave up leaves FL_ETIMEOUT in the

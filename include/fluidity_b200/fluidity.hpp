@@ -281,6 +281,7 @@ struct SplitSolver {
       void* p = nullptr;
       check_cuda(cudaMalloc(&p, (std::size_t)bytes));
       ws_ = std::shared_ptr<void>(p, [](void* q) { cudaFree(q); });
+      check_cuda(cudaMemset(p, 0, (std::size_t)bytes));
       ws_bytes_ = bytes;
     }
     return ws_.get();
