@@ -91,13 +91,13 @@ def workload_config(a):
 
 
 def alternating_transposes(a):
-    """Plane transposes per run of the device-resident loop: the FP64 2-D loop
-    alternates layouts (state in, then back out) when both extents are
-    multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set; "staged"
-    extends it to FP32."""
+    """Plane transposes per run of the device-resident loop: the FP64 HLLC
+    2-D loop alternates layouts (state in, then back out) when both extents
+    are multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set;
+    "staged" extends it to every dtype and flux."""
     mode = os.environ.get("FLUIDITY_B200_SWEEP", "")
     elem = 8 if a.dtype == "f64" else 4
-    on = (mode == "staged") or (mode == "" and a.dtype == "f64")
+    on = (mode == "staged") or (mode == "" and a.dtype == "f64" and a.flux == "hllc")
     return 2 if on and (a.size * elem) % 16 == 0 else 0
 
 
@@ -770,7 +770,59 @@ def measure_adjoint(n=1024, steps=300, directions=16, eps=1e-6):
     out["workload"] = (f"2-D {n}x{n}, rho0 = 1 + 32 Gaussians, p = rho0, at rest, {steps} "
                        f"HLLC/MUSCL steps at CFL 0.7, checkpoint every "
                        f"{math.ceil(math.sqrt(steps))} steps")
+    out["exactness"] = adjoint_exactness()
     return out
+
+
+def adjoint_exactness(n=128, steps=40, directions=4, eps=1e-6):
+    """The FP64 adjoint against an exact reference gradient at a size the CPU
+    evaluates: per seeded direction, <adjoint gradient, v> against the
+    directional derivative in forward-mode dual numbers through the oracle's
+    sweep (oracle/fl_oracle_dual.cpp; the same frozen branches, flattening
+    coefficient and time steps), and the central difference against that
+    exact value.  Where the adjoint matches the exact derivative to rounding,
+    a central difference that misses it is off by its own errors: limiter and
+    wave-speed switches inside +-eps, and round-off in J(u+) - J(u-)."""
+    import numpy as np
+    import torch
+    from oracle import oracle
+    from fluidity_b200.adjoint import (Adjoint, gaussian_density, objective,
+                                       objective_difference, pressure, random_directions,
+                                       rollout, state_from_density)
+    adj = Adjoint((n, n), steps, dtype="f64")
+    with torch.no_grad():
+        p_target = pressure(adj.forward(state_from_density(gaussian_density(n, 2)), 0.7))
+    rho0 = gaussian_density(n, 1).requires_grad_(True)
+    objective(rollout(state_from_density(rho0), adj, 0.7), p_target).backward()
+    grad = rho0.grad.detach()
+    dts = adj.dtdh()
+    r0 = rho0.detach().cpu().numpy()
+    pt = p_target.cpu().numpy()
+    z = np.zeros_like(r0)
+    u0 = np.stack([r0, r0 / 0.4, z, z])
+    t0 = time.perf_counter()
+    ad_err, fd_err = [], []
+    with torch.no_grad():
+        for v in random_directions(r0.size, directions, seed=7):
+            vn = v.cpu().numpy()
+            u, du = oracle.rollout_dual((n, n), u0, np.stack([vn, vn / 0.4, z, z]), 1.4, dts)
+            rho, e, mx, my = u
+            drho, de, dmx, dmy = du
+            ke = 0.5 * (mx * mx + my * my) / rho
+            dke = (mx * dmx + my * dmy) / rho - ke * drho / rho
+            exact = float(np.sum((0.4 * (e - ke) - pt) * 0.4 * (de - dke)))
+            ad = torch.dot(grad, v).item()
+            up = adj.forward(state_from_density(rho0.detach() + eps * v), 0.7, frozen_dtdh=dts)
+            um = adj.forward(state_from_density(rho0.detach() - eps * v), 0.7, frozen_dtdh=dts)
+            fd = objective_difference(up, um, p_target).item() / (2 * eps)
+            ad_err.append(abs(ad - exact) / abs(exact))
+            fd_err.append(abs(fd - exact) / abs(exact))
+    del adj
+    return {"grid": f"{n}x{n}", "steps": steps, "reference": "oracle sweep in forward-mode "
+            "dual numbers (same frozen branches, chi and dt)", "cpu_s": time.perf_counter() - t0,
+            "adjoint_vs_exact_rel": [float(f"{e:.3g}") for e in ad_err],
+            "central_difference_vs_exact_rel": [float(f"{e:.3g}") for e in fd_err],
+            "fd_eps": eps}
 
 
 def measure_multimaterial(nx=2048, ny=1024, steps=500, reinit_every=5, cpu=True):

@@ -726,7 +726,8 @@ int fl_sim_steps(fl_sim* sim, int64_t nsteps, void* stream) {
     SweepParams probe = p;
     probe.in = sim->a;
     probe.out = sim->b;
-    const bool tl = sim->pol.f32 ? loop_transposes_f32(probe) : loop_transposes_f64(probe);
+    const bool tl = sim->pol.f32 ? loop_transposes_f32(probe, sim->pol.flux)
+                                 : loop_transposes_f64(probe, sim->pol.flux);
     if (tl) {
       const int64_t n0 = sim->grid.n[0], n1 = sim->grid.n[1], pt = sim->grid.pitch;
       cudaError_t e = sim->pol.f32 ? launch_transpose<float>(sim->a, sim->b, pt, n0, n1, st)

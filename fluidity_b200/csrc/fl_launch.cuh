@@ -16,7 +16,7 @@ cudaError_t launch_sweep_f32(const SweepParams& p, int dims, int dim, int flux,
 // Whether the device-resident 2-D loop alternates layouts (each sweep reads
 // the state with its own dimension slowest and writes it transposed) for
 // this sweep configuration; p carries the loop's buffers and extents.
-bool loop_transposes_f64(const SweepParams& p);
-bool loop_transposes_f32(const SweepParams& p);
+bool loop_transposes_f64(const SweepParams& p, int flux);
+bool loop_transposes_f32(const SweepParams& p, int flux);
 
 }  // namespace fl

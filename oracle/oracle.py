@@ -92,6 +92,8 @@ def lib():
         L.flo_ls_velocity_f64.argtypes = [C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_int64, C.c_double, C.c_void_p]
         L.flo_ls_project_f64.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
+        L.flo_sweep_dual.argtypes = [P(_Grid), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_double, C.c_double, P(_Policy)]
         L.flo_ls_weno_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double, C.c_void_p,
                                       C.c_void_p]
         L.flo_ls_godunov_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
@@ -233,6 +235,31 @@ def sweep(shape, dim, u, gamma, dtdh, **pol):
     if rc != 0:
         raise ValueError(f"oracle sweep failed ({rc})")
     return out
+
+
+def sweep_dual(shape, dim, u, du, gamma, dtdh, **pol):
+    """One FP64 sweep in forward-mode dual numbers: (sweep(u), derivative of
+    the sweep at u along du), with dtdh held constant, the branches of the
+    primal run and the flattening coefficient taken as a constant."""
+    g = _grid(shape)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    du = np.ascontiguousarray(du, dtype=np.float64)
+    out, dout = np.empty_like(u), np.empty_like(u)
+    p = _policy(**pol)
+    rc = lib().flo_sweep_dual(C.byref(g), dim, _ptr(u), _ptr(du), _ptr(out), _ptr(dout), gamma,
+                              dtdh, C.byref(p))
+    if rc != 0:
+        raise ValueError(f"dual sweep failed ({rc})")
+    return out, dout
+
+
+def rollout_dual(shape, u, du, gamma, dtdh_seq, **pol):
+    """Steps with the given dt/dh sequence (sweeps x, y, z each step), in dual
+    numbers: returns the final state and its derivative along du."""
+    for dtdh in dtdh_seq:
+        for dim in range(len(shape)):
+            u, du = sweep_dual(shape, dim, u, du, gamma, float(dtdh), **pol)
+    return u, du
 
 
 def max_wavespeed(shape, u, gamma):
