@@ -184,11 +184,22 @@ struct fl_adj {
   std::vector<double> dtdh;
   bool have_forward = false;
   int64_t walk_launches = 0;  // forward sweeps launched: the strip counters' parity
+  // a counted sweep failed to launch: it neither took its strips nor cleared
+  // the other counter, so both are re-zeroed before the next pass
+  bool counters_dirty = false;
 };
 
 namespace {
 
 void* state_at(char* base, size_t bytes, int64_t i) { return base + (size_t)i * bytes; }
+
+// Re-zeroes both strip counters on the stream after a failed counted sweep.
+cudaError_t settle_adj_counters(fl_adj* a, cudaStream_t st) {
+  if (!a->counters_dirty) return cudaSuccess;
+  const cudaError_t e = cudaMemsetAsync(a->ctrl->walk_next, 0, sizeof(a->ctrl->walk_next), st);
+  if (e == cudaSuccess) a->counters_dirty = false;
+  return e;
+}
 
 }  // namespace
 
@@ -286,7 +297,8 @@ int fl_adj_forward(fl_adj* a, const void* u0, void* u_final, double cfl, double 
   const size_t sb = a->state_bytes;
   void* cur = state_at(a->work, sb, 0);
   void* nxt = state_at(a->work, sb, 1);
-  cudaError_t e = cudaMemcpyAsync(cur, u0, sb, cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = settle_adj_counters(a, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cur, u0, sb, cudaMemcpyDeviceToDevice, st);
   const bool record = frozen_dtdh == nullptr;
   if (record && e == cudaSuccess) {
     if (!(cfl > 0.0) || !(res > 0.0)) return set_error(kEInval, "cfl and res must be positive");
@@ -346,6 +358,7 @@ int fl_adj_forward(fl_adj* a, const void* u0, void* u_final, double cfl, double 
       p.ws_accum = (record && last) ? &a->ctrl->ws_bits : nullptr;
       p.finalize = (record && last) ? 1 : 0;
       e = fwd_sweep(g, a->policy, p, d, st);
+      if (e != cudaSuccess) a->counters_dirty = true;
       void* t = cur;
       cur = nxt;
       nxt = t;
@@ -387,7 +400,8 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
   const int flux = (int)((a->policy >> 1) & 3u);
   void* la = state_at(a->work, sb, 2);
   void* lb = state_at(a->work, sb, 3);
-  cudaError_t e = cudaMemcpyAsync(la, lambda_final, sb, cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = settle_adj_counters(a, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(la, lambda_final, sb, cudaMemcpyDeviceToDevice, st);
   const int64_t nseg = (a->nsteps + a->interval - 1) / a->interval;
   for (int64_t j = nseg - 1; j >= 0 && e == cudaSuccess; --j) {
     const int64_t k0 = j * a->interval;
@@ -406,6 +420,7 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
         p.walk_next = a->ctrl->walk_next;
         p.walk_slot = (int)(a->walk_launches++ & 1);
         e = fwd_sweep(g, a->policy, p, d, st);
+        if (e != cudaSuccess) a->counters_dirty = true;
       }
     }
     // adjoint sweeps in reverse order

@@ -463,6 +463,7 @@ struct fl_mm {
   fl_grid grid;
   unsigned int* walk_next = nullptr;  // strip counters of the split sweeps (2, device)
   int64_t walk_launches = 0;          // sweeps launched with them: the parity slot
+  bool counters_dirty = false;        // a counted sweep failed: re-zero both first
   uint32_t policy;
   bool f32;
   double gamma[2];
@@ -827,8 +828,14 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
       for (int d = 0; d < 2 && rc == 0; ++d) {
         void* in = m->u[mat][d];
         void* out = m->u[mat][1 - d];
+        if (m->counters_dirty) {
+          const cudaError_t ce = cudaMemsetAsync(m->walk_next, 0, 2 * sizeof(unsigned int), st);
+          if (ce != cudaSuccess) return cuda_err(ce, "fl_mm_steps");
+          m->counters_dirty = false;
+        }
         rc = split_sweep_counted(g, d, in, out, &mm, dtdh, m->policy, 0u, nullptr,
                                  m->walk_next, (int)(m->walk_launches++ & 1), stream);
+        if (rc) m->counters_dirty = true;
       }
       if (rc) return rc;
     }
