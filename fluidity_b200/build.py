@@ -22,9 +22,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
               "-Xptxas", "-O3"]
-# The level-set and ghost-fluid kernels keep every product separately rounded
-# (no FMA contraction), so that they round exactly like the C restatement of
-# the reference's arithmetic; the split-solver kernels contract freely.
+# The level-set velocity, projection and reinitialisation kernels and the
+# ghost-fluid kernels keep every product separately rounded (no FMA
+# contraction), so that they round exactly like the C restatement of the
+# reference's arithmetic; the split-solver kernels and the level-set RK3
+# stages (fl_ls_rk3.cu) contract freely.
 FILE_FLAGS = {"fl_levelset.cu": ["--fmad=false"], "fl_mm.cu": ["--fmad=false"]}
 
 

@@ -9,7 +9,9 @@
 //    evaluators/levelset_hamiltonian.hpp, updaters/runge_kutta_3.hpp); every
 //    stage is one launch over the whole grid, so tile halos always hold the
 //    current stage (the reference's single-launch RK3 keeps stale halos
-//    between stages, scheme/cuda/evolve.cuh:51-157);
+//    between stages, scheme/cuda/evolve.cuh:51-157); the stages are in
+//    fl_ls_rk3.cu, which is built with FMA contraction and agrees with the
+//    reference's operation order to rounding;
 //  * fl_ls_project  : two level sets without overlap or void
 //    (levelset/cuda/levelset_projection.cuh:54-67);
 //  * fl_ls_reinit   : signed-distance reinitialisation: sources next to the
@@ -41,94 +43,7 @@ __device__ __forceinline__ int64_t lmir(int64_t i, int64_t n) {
   return i < 0 ? 0 : (i >= n ? n - 1 : i);
 }
 
-__device__ __forceinline__ double dmax_(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
-
-// WENO-HJ5 combination (weno_hj_5.hpp:85-144)
-__device__ __forceinline__ double weno_diff(double d1, double d2, double d3, double d4,
-                                            double d5) {
-  const double phi_1 = 2.0 * d1 - 7.0 * d2 + 11.0 * d3;
-  const double phi_2 = -d2 + 5.0 * d3 + 2.0 * d4;
-  const double phi_3 = 2.0 * d3 + 5.0 * d4 - d5;
-  const double f1 = 13.0 / 12.0, f2 = 1.0 / 4.0;
-  const double t1 = d1 - 2.0 * d2 + d3, t2 = d1 - 4.0 * d2 + 3.0 * d3;
-  const double t3 = d2 - 2 * d3 + d4, t4 = d2 - d4;
-  const double t5 = d3 - 2.0 * d4 + d5, t6 = 3.0 * d3 - 4.0 * d4 + d5;
-  double a1 = f1 * (t1 * t1) + f2 * (t2 * t2);
-  double a2 = f1 * (t3 * t3) + f2 * (t4 * t4);
-  double a3 = f1 * (t5 * t5) + f2 * (t6 * t6);
-  const double e =
-      10.0e-6 * dmax_(dmax_(dmax_(dmax_(d1 * d1, d2 * d2), d3 * d3), d4 * d4), d5 * d5) + 10.0e-99;
-  const double s1 = a1 + e, s2 = a2 + e, s3 = a3 + e;
-  a1 = 0.1 / (s1 * s1);
-  a2 = 0.6 / (s2 * s2);
-  a3 = 0.3 / (s3 * s3);
-  const double w_denom = (a1 + a2 + a3) * 6.0;
-  return (a1 * phi_1 + a2 * phi_2 + a3 * phi_3) / w_denom;
-}
-
-constexpr int LX = 32, LY = 8, LH = 3;
-constexpr int SX = LX + 2 * LH, SY = LY + 2 * LH;
-
-// One RK3 stage on a 32 x 8 tile staged with a 3-cell halo.
-//   stage 1: out = phi_n - dt H(phi_n)
-//   stage 2: out = 0.75 phi_n + 0.25 (s - dt H(s))
-//   stage 3: out = (1/3) phi_n + (2/3) (s - dt H(s))
-#ifndef FL_LS_RK3_CTAS
-#define FL_LS_RK3_CTAS 4   // 64 registers: 4 CTAs per SM (measured 8% faster than 3 at 74)
-#endif
-template <int STAGE>
-__global__ void __launch_bounds__(LX * LY, FL_LS_RK3_CTAS) ls_rk3_kernel(const double* __restrict__ phi_n,
-                                                         const double* __restrict__ s,
-                                                         const double* __restrict__ vel,
-                                                         double dt, double h, int64_t nx,
-                                                         int64_t ny, double* __restrict__ out) {
-  __shared__ double tile[SY][SX + 1];
-  const int64_t x0 = (int64_t)blockIdx.x * LX, y0 = (int64_t)blockIdx.y * LY;
-  const double* src = (STAGE == 1) ? phi_n : s;
-  for (int i = threadIdx.x; i < SX * SY; i += LX * LY) {
-    const int lx = i % SX, ly = i / SX;
-    tile[ly][lx] = src[lmir(y0 - LH + ly, ny) * nx + lmir(x0 - LH + lx, nx)];
-  }
-  __syncthreads();
-  const int tx = threadIdx.x % LX, ty = threadIdx.x / LX;
-  const int64_t x = x0 + tx, y = y0 + ty;
-  if (x >= nx || y >= ny) return;
-  const int cx = tx + LH, cy = ty + LH;
-  const int64_t i = y * nx + x;
-  const double v = vel[i];
-  const double h1 = 1.0 / h;
-  double r = 0.0;
-#pragma unroll
-  for (int d = 0; d < 2; ++d) {
-    double p[7];
-#pragma unroll
-    for (int k = -3; k <= 3; ++k) p[k + 3] = (d == 0) ? tile[cy][cx + k] : tile[cy + k][cx];
-    const double bk = weno_diff(h1 * (p[1] - p[0]), h1 * (p[2] - p[1]), h1 * (p[3] - p[2]),
-                                h1 * (p[4] - p[3]), h1 * (p[5] - p[4]));
-    const double fw = weno_diff(h1 * (p[6] - p[5]), h1 * (p[5] - p[4]), h1 * (p[4] - p[3]),
-                                h1 * (p[3] - p[2]), h1 * (p[2] - p[1]));
-    double b, w;
-    if (v <= 0.0) {
-      b = dmax_(bk, 0.0);
-      w = dmin_(fw, 0.0);
-    } else {
-      b = dmin_(bk, 0.0);
-      w = dmax_(fw, 0.0);
-    }
-    r += dmax_(b * b, w * w);
-  }
-  const double H = v * sqrt(r);
-  const double cur = tile[cy][cx];
-  if (STAGE == 1) {
-    out[i] = cur - dt * H;
-  } else if (STAGE == 2) {
-    out[i] = 0.75 * phi_n[i] + 0.25 * (cur - dt * H);
-  } else {
-    const double f13 = 1.0 / 3.0, f23 = 2.0 * f13;
-    out[i] = (f13 * phi_n[i]) + (f23 * (cur - dt * H));
-  }
-}
 
 template <typename T>
 __global__ void ls_velocity_kernel(int64_t nx, int64_t ny, int nmat, const double* phi0,
@@ -311,6 +226,12 @@ unsigned grid1d(int64_t n) {
 }
 
 }  // namespace
+
+// The three RK3 stages of fl_ls_advect (fl_ls_rk3.cu, built with FMA
+// contraction; the kernels here are built without it).
+cudaError_t launch_ls_rk3(const double* phi, const double* vel, double dt, double h, int64_t nx,
+                          int64_t ny, double* s1, double* s2, double* out, cudaStream_t st);
+
 }  // namespace fl
 
 using namespace fl;
@@ -367,12 +288,7 @@ int fl_ls_advect(const fl_grid* grid, const double* phi, const double* vel, doub
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t nx = grid->n[0], ny = grid->n[1], n = nx * ny;
   double* s1 = static_cast<double*>(workspace);
-  double* s2 = s1 + n;
-  const dim3 g((unsigned)((nx + LX - 1) / LX), (unsigned)((ny + LY - 1) / LY));
-  ls_rk3_kernel<1><<<g, LX * LY, 0, st>>>(phi, nullptr, vel, dt, h, nx, ny, s1);
-  ls_rk3_kernel<2><<<g, LX * LY, 0, st>>>(phi, s1, vel, dt, h, nx, ny, s2);
-  ls_rk3_kernel<3><<<g, LX * LY, 0, st>>>(phi, s2, vel, dt, h, nx, ny, out);
-  cudaError_t e = cudaGetLastError();
+  const cudaError_t e = launch_ls_rk3(phi, vel, dt, h, nx, ny, s1, s1 + n, out, st);
   if (e != cudaSuccess) return set_error(kECuda, "fl_ls_advect: %s", cudaGetErrorString(e));
   return kOk;
 }

@@ -4,9 +4,11 @@ CPU, then the CUDA kernels against the oracle on the same seeded inputs.
 Reference: levelset/cuda/velocity_initialization.cuh, scheme/cuda/evolve.cuh
 with scheme/updaters/runge_kutta_3.hpp and scheme/stencils/weno_hj_5.hpp,
 levelset/cuda/levelset_projection.cuh, scheme/cuda/fast_iterative_method.cuh.
-Bit-exactness: the level-set kernels are compiled without FMA contraction
-and use IEEE division and square root, so advection, velocities and the
-projection match the oracle bit for bit.  The reinitialisation relaxes in a
+Bit-exactness: the velocity and projection kernels are compiled without FMA
+contraction and use IEEE division and square root, so they match the oracle
+bit for bit.  The RK3 advection contracts into FMAs and normalises the WENO
+weights with one reciprocal per derivative; it agrees with the oracle to
+1e-12 of max |phi|, one step or twenty.  The reinitialisation relaxes in a
 different order (16x16 tiles against whole-grid Jacobi sweeps); its fixed
 point agrees to 1e-12 of max |phi|.
 """
@@ -118,6 +120,14 @@ def test_oracle_velocity_uniform(oracle):
 
 # ---- CUDA kernels vs the oracle -----------------------------------------------
 
+# The advection's bar against the oracle: max |got - want| over max |want|.
+ADVECT_TOL = 1e-12
+
+
+def _maxrel(got, want):
+    return float(np.max(np.abs(got - want)) / np.max(np.abs(want)))
+
+
 def _ops(shape):
     from fluidity_b200.levelset import LevelSetOps
     return LevelSetOps(shape)
@@ -133,7 +143,9 @@ def test_advect_matches_oracle(cuda, oracle, nx, ny, seed):
     want = oracle.ls_advect(nx, ny, phi, vel, dt, h)
     ops = _ops((nx, ny))
     got = ops.advect(torch.tensor(phi, device=cuda), torch.tensor(vel, device=cuda), dt, h)
-    assert np.array_equal(got.cpu().numpy(), want)
+    # the RK3 stages contract products into FMAs and normalise the WENO
+    # weights with one reciprocal: rounding-level agreement
+    assert _maxrel(got.cpu().numpy(), want) <= ADVECT_TOL
 
 
 @pytest.mark.gpu
@@ -152,7 +164,7 @@ def test_advect_many_steps(cuda, oracle):
         want = oracle.ls_advect(nx, ny, want, vel, dt, h)
         ops.advect(a, v, dt, h, out=b)
         a, b = b, a
-    assert np.array_equal(a.cpu().numpy(), want)
+    assert _maxrel(a.cpu().numpy(), want) <= ADVECT_TOL
 
 
 @pytest.mark.gpu

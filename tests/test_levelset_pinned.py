@@ -14,8 +14,9 @@ reference's own level-set functors, through tests/golden/levelset.npz
   math::interp probes, the rotation into the normal, the two-material HLLC
   star state and the rotation back (ghost_fluid/riemann_ghost_fluid.hpp:70-190).
 
-The CUDA level-set kernels are held to this oracle bit for bit
-(tests/test_levelset.py), so they are pinned to the reference through it.
+The CUDA level-set kernels are held to this oracle (tests/test_levelset.py:
+velocities and projection bit for bit, the RK3 advection to 1e-12 of max
+|phi|), so they are pinned to the reference through it.
 Where the reference-functor library is present (it is built from the
 reference's sources), the same comparisons also run on fresh seeded fields.
 """
