@@ -874,17 +874,25 @@ def measure_multimaterial(nx=2048, ny=1024, steps=500, reinit_every=5, cpu=True)
         a0 = O.mm_set_states(a0, spec["shock_phi"], spec["shocked"], g0)
         a1 = O.mm_set_states(np.zeros((4, n), np.float32), -np.ones(n), spec["bubble"], g1)
         p0h, p1h = spec["phi0"], spec["phi1"]
-        t0 = _t.perf_counter()
-        k = 0
-        while k < 2:
-            a0, a1, p0h, p1h, _ = O.mm_step(nx, ny, spec["h"], spec["gammas"], 0.6, a0, a1, p0h,
-                                            p1h, reinit=False)
-            k += 1
-        sec = _t.perf_counter() - t0
-        out["cpu_baseline"] = {"value": cells * k / sec, "unit": "cell-updates/s", "cores": 1,
-                               "kind": "port",
-                               "sample": f"{k} steps (no reinitialisation) of the same "
-                                         f"workload in the C oracle, 1 thread, {sec:.1f} s"}
+        # one reinitialisation cycle: reinit_every steps, the last followed
+        # by the reinitialisation of level set 0; level set 1 takes its
+        # negation (the projection leaves phi1 = -phi0 and the
+        # reinitialisation is odd), as the GPU loop does
+        with O.threaded():
+            cores = O.threads()
+            t0 = _t.perf_counter()
+            for _ in range(reinit_every):
+                a0, a1, p0h, p1h, _dt = O.mm_step(nx, ny, spec["h"], spec["gammas"], 0.6, a0,
+                                                  a1, p0h, p1h, reinit=False)
+            p0h, sweeps = O.ls_reinit(nx, ny, p0h, spec["h"])
+            p1h = -p0h
+            sec = _t.perf_counter() - t0
+        k = reinit_every
+        out["cpu_baseline"] = {"value": cells * k / sec, "unit": "cell-updates/s",
+                               "cores": cores, "kind": "port",
+                               "sample": f"{k} steps and one reinitialisation ({sweeps} Jacobi "
+                                         f"sweeps) of the same workload in the C oracle, OpenMP "
+                                         f"over rows, {cores} threads, {sec:.1f} s"}
     return out
 
 

@@ -19,6 +19,10 @@
  * interface-normal velocity -- are pinned bit for bit to them through
  * tests/golden/levelset.npz (tests/test_levelset_pinned.py).  The CUDA
  * kernels are checked against this file.
+ *
+ * The row loops carry OpenMP pragmas: liboracle_omp.so (-fopenmp) shares rows
+ * among threads for the timed CPU baseline; every cell is computed exactly
+ * as in the single-threaded liboracle.so the tests use.
  */
 #include <float.h>
 #include <math.h>
@@ -113,11 +117,13 @@ static double hamiltonian(const double* f, int64_t nx, int64_t ny, int64_t x, in
  * freshly mirrored ghosts. */
 void flo_ls_rk3_stages_f64(int64_t nx, int64_t ny, const double* phi, const double* vel,
                            double dt, double h, double* s1, double* s2) {
+#pragma omp parallel for schedule(static)
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
       s1[i] = phi[i] - dt * hamiltonian(phi, nx, ny, x, y, h, vel[i]);
     }
+#pragma omp parallel for schedule(static)
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
@@ -134,6 +140,7 @@ void flo_ls_advect_f64(int64_t nx, int64_t ny, const double* phi, const double* 
   double* s2 = (double*)malloc(sizeof(double) * n);
   flo_ls_rk3_stages_f64(nx, ny, phi, vel, dt, h, s1, s2);
   const double f13 = 1.0 / 3.0, f23 = 2.0 * f13;
+#pragma omp parallel for schedule(static)
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
@@ -151,6 +158,7 @@ void flo_ls_advect_f64(int64_t nx, int64_t ny, const double* phi, const double* 
  * contains the cell.  states: per material (rho, E, m_x, m_y) planes. */
 void flo_ls_velocity_f64(int64_t nx, int64_t ny, int nmat, const double* const* phis,
                          const double* const* states, int64_t pitch, double h, double* vel) {
+#pragma omp parallel for schedule(static)
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
@@ -175,6 +183,7 @@ void flo_ls_velocity_f64(int64_t nx, int64_t ny, int nmat, const double* const* 
 /* Two level sets: remove overlaps and voids
  * (levelset/cuda/levelset_projection.cuh:54-67). */
 void flo_ls_project_f64(int64_t n, double* a, double* b) {
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) {
     const double avg = 0.5 * (a[i] + b[i]);
     a[i] -= avg;
@@ -248,6 +257,7 @@ int flo_ls_reinit_f64(int64_t nx, int64_t ny, const double* phi, double h, doubl
                       int max_sweeps) {
   const int64_t n = nx * ny;
   unsigned char* src = (unsigned char*)calloc((size_t)n, 1);
+#pragma omp parallel for schedule(static)
   for (int64_t y = 0; y < ny; ++y)
     for (int64_t x = 0; x < nx; ++x) {
       const int64_t i = y * nx + x;
@@ -267,6 +277,7 @@ int flo_ls_reinit_f64(int64_t nx, int64_t ny, const double* phi, double h, doubl
   int sweeps = 0;
   for (; sweeps < max_sweeps; ++sweeps) {
     int changed = 0;
+#pragma omp parallel for schedule(static) reduction(| : changed)
     for (int64_t y = 0; y < ny; ++y)
       for (int64_t x = 0; x < nx; ++x) {
         const int64_t i = y * nx + x;
@@ -278,6 +289,7 @@ int flo_ls_reinit_f64(int64_t nx, int64_t ny, const double* phi, double h, doubl
     memcpy(out, nxt, sizeof(double) * n);
     if (!changed) break;
   }
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) out[i] = (double)sgn(phi[i]) * fabs(out[i]);
   free(nxt);
   free(src);

@@ -268,6 +268,7 @@ int flo_mm_extrapolate(int64_t nx, int64_t ny, int64_t pitch, double h, double* 
   for (; it < max_iters;) {
     double worst = 0.0;
     int nan_seen = 0;
+#pragma omp parallel for schedule(static) reduction(max : worst) reduction(| : nan_seen)
     for (int64_t y = 0; y < ny; ++y)
       for (int64_t x = 0; x < nx; ++x) {
         const int64_t i = y * nx + x;

@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE ONLY.  Imported by tests/, ``__graft_entry__.smoke()`` and
 bench.py's CPU-baseline leg as the checker; the product never imports it.
 
 * ``liboracle.so`` -- the plain-C restatement (fl_oracle.c) of the reference's
-  split-solver arithmetic (FP64 and FP32).
+  split-solver arithmetic (FP64 and FP32); ``liboracle_omp.so`` is the same
+  sources with OpenMP, for the timed CPU baseline (``threaded()``).
 * ``_ref/libfluidity_ref.so`` -- the reference's own functors driven by
   ref_driver.cpp (FP64 only: the reference's MUSCL reconstructor does not
   compile for float, reconstruction/muscl_reconstructor.hpp:112,155).
@@ -23,6 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
+ORACLE_OMP_SO = os.path.join(HERE, "liboracle_omp.so")
 REF_SO = os.path.join(HERE, "_ref", "libfluidity_ref.so")
 
 FLUX = {"hllc": 0, "force": 1, "lf": 2, "richtmyer": 3}
@@ -50,16 +52,38 @@ def build(ref_root: str | None = None) -> None:
                        stdout=subprocess.DEVNULL)
 
 
-_lib = None
+_libs: dict = {}
+_threaded = False
 _ref = None
 
 
+@contextlib.contextmanager
+def threaded():
+    """Within the block the oracle runs from liboracle_omp.so: the same
+    sources built with -fopenmp, rows and sweep lines shared among threads
+    (OMP_NUM_THREADS, default all host cores), every cell computed as in the
+    single-threaded build.  Used to time the CPU baseline."""
+    global _threaded
+    old = _threaded
+    _threaded = True
+    try:
+        yield lib()
+    finally:
+        _threaded = old
+
+
+def threads() -> int:
+    """Threads the threaded build uses."""
+    return int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or (os.cpu_count() or 1)
+
+
 def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(ORACLE_SO):
+    path = ORACLE_OMP_SO if _threaded else ORACLE_SO
+    L = _libs.get(path)
+    if L is None:
+        if not os.path.exists(path):
             subprocess.run(["make", "-s", "-C", HERE], check=True)
-        L = C.CDLL(ORACLE_SO)
+        L = C.CDLL(path)
         P = C.POINTER
         L.flo_sweep_f64.argtypes = [P(_Grid), C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_double, P(_Policy)]
@@ -132,8 +156,8 @@ def lib():
         L.flo_mm_combine.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         L.flo_set_p_inf.argtypes = [C.c_double]
         L.flo_get_p_inf.restype = C.c_double
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return L
 
 
 def ref_available() -> bool:
