@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(compile_one, sources()))
     tmp = lib + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")

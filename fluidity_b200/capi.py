@@ -129,6 +129,18 @@ PROTOTYPES = {
     "fl_sim_finalize": (C.c_int, [_P, C.c_int, _P]),
     "fl_sim_status": (C.c_int, [_P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int), C.POINTER(_P)]),
+    "fl_slab_nccl_available": (C.c_int, []),
+    "fl_slab_nccl_id": (C.c_int, [_P]),
+    "fl_slab_create_nccl": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,
+                                      C.c_int64, C.c_int64, _P, C.c_int, C.c_int]),
+    "fl_slab_create_local": (C.c_int, [C.POINTER(_P), _G, C.c_double, C.c_uint32, C.c_uint32,
+                                       C.c_int64, C.c_int64]),
+    "fl_slab_set_material": (C.c_int, [_P, C.POINTER(Material)]),
+    "fl_slab_sim": (C.c_int, [_P, C.POINTER(_P)]),
+    "fl_slab_begin": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P), C.POINTER(_P), C.c_double,
+                                C.c_double, C.c_double, C.c_int64, _P]),
+    "fl_slab_steps": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int64, _P]),
+    "fl_slab_destroy": (C.c_int, [_P]),
     "fl_simulate": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int64, _P,
                               C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(_P)]),
     "fl_simulate_noalloc": (C.c_int, [_G, C.c_double, C.c_uint32, C.c_uint32, _P, _P, C.c_double,

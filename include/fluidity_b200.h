@@ -272,6 +272,44 @@ int fl_sim_finalize(fl_sim* sim, int advance, void* stream);
 int fl_sim_status(fl_sim* sim, void* stream, int64_t* iters, double* run_time,
                   int* done, void** result);
 
+/* ---- the decomposed step below the host (no reference counterpart: the
+ * reference runs one GPU).  A slab is a 2-D local grid whose rows
+ * [own_lo, own_hi) are its own, with ghost rows facing its neighbours (at
+ * least 4 on each side that has one).  fl_slab_steps enqueues whole steps on
+ * one stream -- exchange 3 ghost rows, x sweep, exchange 4 ghost rows, y
+ * sweep, MAX of the wavespeed over the slabs, finalize -- and reads nothing
+ * back, so the steps can be captured in a CUDA graph.  The result equals the
+ * undivided run bit for bit.
+ *
+ * NCCL transport, one rank (process, GPU) per slab: rank 0 makes a 128-byte
+ * id with fl_slab_nccl_id and hands it to every rank, which calls
+ * fl_slab_create_nccl (collective; world 1 needs no id, and with one makes
+ * a communicator of one rank).  The exchange is
+ * ncclSend / ncclRecv into local ghost rows, the maximum one 64-bit
+ * ncclAllReduce.  libnccl.so.2 is loaded at run time; fl_slab_nccl_available
+ * says whether it could be.
+ *
+ * In-process transport: slabs made with fl_slab_create_local and stepped
+ * together, bottom to top, in one fl_slab_begin / fl_slab_steps call (one
+ * stream; neighbours are the adjacent array entries; at most 16). */
+typedef struct fl_slab fl_slab;
+int fl_slab_nccl_available(void);
+int fl_slab_nccl_id(void* id);
+int fl_slab_create_nccl(fl_slab** slab, const fl_grid* grid, double gamma, uint32_t policy,
+                        uint32_t boundary_mask, int64_t own_lo, int64_t own_hi,
+                        const void* nccl_id, int world, int rank);
+int fl_slab_create_local(fl_slab** slab, const fl_grid* grid, double gamma, uint32_t policy,
+                         uint32_t boundary_mask, int64_t own_lo, int64_t own_hi);
+int fl_slab_set_material(fl_slab* slab, const fl_material* mat);
+/* The slab's time loop, for fl_sim_status. */
+int fl_slab_sim(fl_slab* slab, fl_sim** sim);
+/* a[i], b[i]: slab i's state buffers (a holds its initial state, ghost rows
+ * included); then the initial wavespeed maximum and time step. */
+int fl_slab_begin(fl_slab* const* slabs, int count, void* const* a, void* const* b,
+                  double cfl, double res, double sim_time, int64_t max_iters, void* stream);
+int fl_slab_steps(fl_slab* const* slabs, int count, int64_t nsteps, void* stream);
+int fl_slab_destroy(fl_slab* slab);
+
 /* Convenience: begin + steps in chunks until done, like simulate(). */
 int fl_simulate(fl_sim* sim, void* a, void* b, double cfl, double res,
                 double sim_time, int64_t max_iters, void* stream,

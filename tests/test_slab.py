@@ -80,12 +80,40 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, shape, u0, nsteps, out_path):
+def _poisoning_runner(SlabRunner, ROWS_X, ROWS_Y):
+    """SlabRunner whose x sweep sees a strong pressure jump (rho 1, E 1e4,
+    at rest) in every ghost row the x exchange does not refresh: the
+    flattening coefficient reacts to it, so the result can only stay exact if
+    the x sweep never reads those rows.  (NaN would not do: the coefficient's
+    comparisons are false for NaN and leave it unflattened.)"""
+
+    class Poisoned(SlabRunner):
+        def step(self):
+            a, b = self.ops.buffers
+            L, nx = self.L, self.L.nx
+            self.exchange(a, ROWS_X)
+            for lo, hi in ((0, L.own[0] - ROWS_X), (L.own[1] + ROWS_X, L.rows)):
+                if hi > lo:
+                    a[:, lo * nx:hi * nx] = 0.0
+                    a[0, lo * nx:hi * nx] = 1.0
+                    a[1, lo * nx:hi * nx] = 1e4
+            self.ops.sweep(0)
+            self.exchange(b, ROWS_Y)
+            self.ops.sweep(1)
+            self._reduce_ws()
+            self.ops.finalize(advance=True)
+
+    return Poisoned
+
+
+def _rank_main(rank, world, port, shape, u0, nsteps, out_path, poison=False):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        from fluidity_b200.slab import SlabLayout, SlabRunner
+        from fluidity_b200.slab import ROWS_X, ROWS_Y, SlabLayout, SlabRunner
+        if poison:
+            SlabRunner = _poisoning_runner(SlabRunner, ROWS_X, ROWS_Y)
         L = SlabLayout(shape, world, rank)
         ops = OracleSlabOps(L)
         a = torch.from_numpy(np.ascontiguousarray(u0[:, L.global_slice()]))
@@ -102,13 +130,13 @@ def _rank_main(rank, world, port, shape, u0, nsteps, out_path):
         dist.destroy_process_group()
 
 
-def _run(world, shape, nsteps, tmp_path):
+def _run(world, shape, nsteps, tmp_path, poison=False):
     from _util import random_prim
     from oracle import oracle
     prim = random_prim(shape, 5, smooth=True, mild=True)
     u0 = oracle.prim_to_cons(prim, GAMMA)
     out = str(tmp_path / f"slab_{world}.npy")
-    mp.start_processes(_rank_main, args=(world, _free_port(), shape, u0, nsteps, out),
+    mp.start_processes(_rank_main, args=(world, _free_port(), shape, u0, nsteps, out, poison),
                        nprocs=world, join=True, start_method="spawn")
     parts = np.load(out, allow_pickle=True)
     got = np.zeros_like(u0)
@@ -126,6 +154,16 @@ def _run(world, shape, nsteps, tmp_path):
 @pytest.mark.parametrize("world", [2, 3])
 def test_slab_decomposition_matches_undivided_run(world, tmp_path):
     got, want = _run(world, (24, 37), 6, tmp_path)
+    assert np.array_equal(got, want)
+
+
+def test_x_sweep_reads_three_ghost_rows(tmp_path):
+    """3 ghost rows before the x sweep are enough: with the fourth poisoned
+    before every x sweep the decomposed run still equals the undivided one.
+    (3 across and 4 along are the stencil's bounds; on random states a
+    changed row was seen to move x-sweep results at most 2 rows away and
+    y-sweep results at most 3.)"""
+    got, want = _run(3, (24, 37), 5, tmp_path, poison=True)
     assert np.array_equal(got, want)
 
 
