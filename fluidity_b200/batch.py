@@ -37,6 +37,33 @@ def batched_workload(seed: int = 3, n1d: int = 3584, n2d: int = 512, lo1=64, hi1
     return problems
 
 
+def problem_cost(shape) -> int:
+    """Work of one time step of a problem: cells x sweeps (one sweep per
+    dimension).  For a run of a fixed step count this orders problems by
+    their device time."""
+    return int(np.prod(shape)) * len(shape)
+
+
+def partition_problems(problems, world: int) -> list[list[int]]:
+    """Cost-balanced split of a problem list over `world` ranks (one GPU
+    each), with no communication: every rank computes the same split.
+
+    Greedy longest-first: problems in decreasing cost (ties by index) go
+    one by one to the rank with the least cost so far (ties to the lowest
+    rank).  The largest load exceeds the smallest by at most one problem's
+    cost.  Returns, per rank, the problem indices in increasing order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(problems)), key=lambda i: (-problem_cost(problems[i][0]), i))
+    load = [0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += problem_cost(problems[i][0])
+    return [sorted(p) for p in parts]
+
+
 class Batch:
     """A set of problems, their arenas and the fl_batch handle."""
 
@@ -76,6 +103,14 @@ class Batch:
         if self.p_inf != 0.0:
             mat = capi.Material(float(gamma), self.p_inf)
             capi.check(self.lib.fl_batch_set_material(h, C.byref(mat)), self.lib)
+
+    @classmethod
+    def shard(cls, problems, world: int, rank: int, **kw):
+        """This rank's share of a batch split over `world` GPUs by
+        partition_problems: (Batch of the share, the share's indices into
+        `problems`).  No collective is involved."""
+        idx = partition_problems(problems, world)[rank]
+        return cls([problems[i] for i in idx], **kw), idx
 
     def __del__(self):
         h = getattr(self, "handle", None)
