@@ -93,7 +93,8 @@ def test_sharded_batch_on_two_ranks_matches_serial(tmp_path):
 @pytest.mark.parametrize("world", [2, 3])
 def test_shards_on_one_gpu_match_whole_batch(cuda, world):
     """Batch.shard for every rank, run one after another on this GPU: each
-    problem's final state and step count equal those of the whole batch."""
+    problem's final state, step count and time equal those of the whole
+    batch (NaN where the whole batch has NaN)."""
     import torch
     from fluidity_b200.batch import Batch
     probs = batched_workload(seed=7, n1d=40, n2d=8, lo1=16, hi1=2000, lo2=16, hi2=96)
@@ -103,7 +104,8 @@ def test_shards_on_one_gpu_match_whole_batch(cuda, world):
         b.fill()
         b.begin(0.8, 1e30, steps)
         b.steps(steps)
-        it, rt, done, _ = b.status()
+        # some random problems of this workload blow up: compared as they are
+        it, rt, done, _ = b.status(allow_nan=True)
         torch.cuda.synchronize()
         return [(b.state(k).cpu().numpy(), it[k], rt[k]) for k in range(len(b.problems))]
 
@@ -113,7 +115,7 @@ def test_shards_on_one_gpu_match_whole_batch(cuda, world):
         b, idx = Batch.shard(probs, world, r, dtype="f64")
         for k, (u, it, rt) in zip(idx, run(b)):
             wu, wit, wrt = whole[k]
-            assert it == wit == steps and rt == wrt
-            assert np.array_equal(u, wu)
+            assert it == wit and (rt == wrt or (np.isnan(rt) and np.isnan(wrt)))
+            assert np.array_equal(u, wu, equal_nan=True)
         seen += idx
     assert sorted(seen) == list(range(len(probs)))
