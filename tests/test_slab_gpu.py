@@ -172,3 +172,20 @@ def test_native_slab_rejects_thin_ghosts(cuda):
     assert lib.fl_slab_create_nccl(C.byref(h), C.byref(g), 1.4, 0, 0, 3, 40, idbuf, 2, 1) \
         == capi.FL_EINVAL
     assert b"ghost rows" in lib.fl_last_error_string()
+
+
+@pytest.mark.parametrize("impl", ["native", "python"])
+def test_bench_slab_path_one_rank(cuda, capsys, impl):
+    """bench.py's multi-GPU path (run_slabs) on one rank and a small grid:
+    the native slab step with a one-rank NCCL communicator, or the Python
+    schedule, prints a complete line."""
+    import argparse
+    import json
+    import bench
+    a = argparse.Namespace(size=64, time_steps=4, dtype="f64", flux="hllc", warmup=3, steps=2,
+                           gpus=1, slab_impl=impl, impl="ours")
+    bench.run_slabs(a, 1, 0, 0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["value"] > 0 and line["n_gpus"] == 1
+    want = "fl_slab_steps (NCCL)" if impl == "native" else "Python schedule over fl_sim_sweep"
+    assert line["config"]["slab_step"] == want
