@@ -804,27 +804,46 @@ def adjoint_exactness(n=128, steps=40, directions=4, eps=1e-6):
     z = np.zeros_like(r0)
     u0 = np.stack([r0, r0 / 0.4, z, z])
     t0 = time.perf_counter()
-    ad_err, fd_err = [], []
+    ad_err, fd_err, fd_chi_err, chi_terms, flips = [], [], [], [], []
+
+    def directional(u, du):
+        rho, e, mx, my = u
+        drho, de, dmx, dmy = du
+        ke = 0.5 * (mx * mx + my * my) / rho
+        dke = (mx * dmx + my * dmy) / rho - ke * drho / rho
+        return float(np.sum((0.4 * (e - ke) - pt) * 0.4 * (de - dke)))
+
     with torch.no_grad():
         for v in random_directions(r0.size, directions, seed=7):
             vn = v.cpu().numpy()
-            u, du = oracle.rollout_dual((n, n), u0, np.stack([vn, vn / 0.4, z, z]), 1.4, dts)
-            rho, e, mx, my = u
-            drho, de, dmx, dmy = du
-            ke = 0.5 * (mx * mx + my * my) / rho
-            dke = (mx * dmx + my * dmy) / rho - ke * drho / rho
-            exact = float(np.sum((0.4 * (e - ke) - pt) * 0.4 * (de - dke)))
+            dv = np.stack([vn, vn / 0.4, z, z])
+            exact = directional(*oracle.rollout_dual((n, n), u0, dv, 1.4, dts))
+            exact_chi = directional(*oracle.rollout_dual((n, n), u0, dv, 1.4, dts,
+                                                         chi_diff=True))
+            _, tp = oracle.rollout_trace((n, n), u0 + eps * dv, 1.4, dts)
+            _, tm = oracle.rollout_trace((n, n), u0 - eps * dv, 1.4, dts)
             ad = torch.dot(grad, v).item()
             up = adj.forward(state_from_density(rho0.detach() + eps * v), 0.7, frozen_dtdh=dts)
             um = adj.forward(state_from_density(rho0.detach() - eps * v), 0.7, frozen_dtdh=dts)
             fd = objective_difference(up, um, p_target).item() / (2 * eps)
             ad_err.append(abs(ad - exact) / abs(exact))
             fd_err.append(abs(fd - exact) / abs(exact))
+            fd_chi_err.append(abs(fd - exact_chi) / abs(exact_chi))
+            chi_terms.append(abs(exact_chi - exact) / abs(exact))
+            flips.append(oracle.branch_flips(tp, tm))
     del adj
+    g3 = lambda xs: [float(f"{e:.3g}") for e in xs]
     return {"grid": f"{n}x{n}", "steps": steps, "reference": "oracle sweep in forward-mode "
             "dual numbers (same frozen branches, chi and dt)", "cpu_s": time.perf_counter() - t0,
-            "adjoint_vs_exact_rel": [float(f"{e:.3g}") for e in ad_err],
-            "central_difference_vs_exact_rel": [float(f"{e:.3g}") for e in fd_err],
+            "adjoint_vs_exact_rel": g3(ad_err),
+            "central_difference_vs_exact_rel": g3(fd_err),
+            "central_difference_vs_exact_with_chi_rel": g3(fd_chi_err),
+            "chi_terms_rel": g3(chi_terms),
+            "branch_flips_between_u_plus_and_u_minus": flips,
+            "reading": "the adjoint equals the frozen-chi derivative to rounding; a central "
+                       "difference straddling no branch flip equals the chi-differentiated "
+                       "derivative (tests/test_branch_flips.py), and chi_terms_rel is what "
+                       "freezing chi leaves out",
             "fd_eps": eps}
 
 

@@ -21,15 +21,41 @@ static double flo_p_inf_ = 0.0;
 void flo_set_p_inf(double p_inf) { flo_p_inf_ = p_inf; }
 double flo_get_p_inf(void) { return flo_p_inf_; }
 
+/* Branch trace of the FP64 sweep (flo_sweep_trace_f64): while flo_trace_out
+ * is set, every branch decision of an evolved cell or a face folds into a
+ * per-thread running hash, stored per cell and face of each line.  Two runs
+ * whose hashes differ at an entry took different branches there. */
+static uint64_t* flo_trace_out = NULL;
+static _Thread_local uint64_t flo_trace_h = 0;
+static inline int flo_trace_bit(int c) {
+  if (flo_trace_out) flo_trace_h = (flo_trace_h ^ (uint64_t)(c != 0)) * 0x100000001b3ull + 1u;
+  return c;
+}
+
+/* |x| with its sign decision traced (its derivative switches sign there) */
+static inline double flo_trace_fabs(double x) {
+  (void)flo_trace_bit(x < 0.0);
+  return fabs(x);
+}
+
 #define T double
 #define SFX _f64
 #define SQRT(x) sqrt(x)
-#define FABS(x) fabs(x)
+#define FABS(x) flo_trace_fabs(x)
+#define FLO_BR(c) flo_trace_bit(c)
+#define FLO_TRACE_BEGIN() (flo_trace_h = 0)
+#define FLO_TRACE_END(slot) \
+  do {                      \
+    if (flo_trace_out) flo_trace_out[(slot)] = flo_trace_h; \
+  } while (0)
 #include "fl_oracle_impl.inc"
 #undef T
 #undef SFX
 #undef SQRT
 #undef FABS
+#undef FLO_BR
+#undef FLO_TRACE_BEGIN
+#undef FLO_TRACE_END
 
 #define T float
 #define SFX _f32
@@ -55,6 +81,15 @@ int flo_sweep_f64(const flo_grid* g, int dim, const double* in, double* out,
                   double gamma, double dtdh, const flo_policy* pol) {
   if (!check_grid(g)) return -1;
   return sweep_impl_f64(g, dim, in, out, gamma, dtdh, pol);
+}
+
+int flo_sweep_trace_f64(const flo_grid* g, int dim, const double* in, double* out,
+                        double gamma, double dtdh, const flo_policy* pol, uint64_t* trace) {
+  if (!check_grid(g) || !trace) return -1;
+  flo_trace_out = trace;
+  const int rc = sweep_impl_f64(g, dim, in, out, gamma, dtdh, pol);
+  flo_trace_out = NULL;
+  return rc;
 }
 
 int flo_sweep_f32(const flo_grid* g, int dim, const float* in, float* out,

@@ -62,6 +62,27 @@ int flo_sweep_f64(const flo_grid* g, int dim, const double* in, double* out,
 int flo_sweep_f32(const flo_grid* g, int dim, const float* in, float* out,
                   float gamma, float dtdh, const flo_policy* pol);
 
+/* flo_sweep_f64 that also records the branch decisions (limiter cases, the
+ * flattening test and clamps, HLLC's pressure clamp, wave and region tests)
+ * as one hash per evolved cell and per face: trace[l * (2n + 3) + i + 1] for
+ * the evolved cell i = -1..n of line l, trace[l * (2n + 3) + n + 2 + f] for
+ * face f = 0..n (n = cells along dim; lines in the sweep's order).  Two
+ * sweeps took the same branches at an entry iff the hashes agree there
+ * (up to hash collisions). */
+/* One FP64 sweep in forward-mode dual numbers (fl_oracle_dual.cpp):
+ * out = sweep(in), out_dot = d sweep(in) [in_dot] with dtdh constant and the
+ * branches of the values.  flo_sweep_dual takes the flattening coefficient
+ * as a constant; flo_sweep_dual_chi differentiates it through its ramp. */
+int flo_sweep_dual(const flo_grid* g, int dim, const double* in, const double* in_dot,
+                   double* out, double* out_dot, double gamma, double dtdh,
+                   const flo_policy* pol);
+int flo_sweep_dual_chi(const flo_grid* g, int dim, const double* in, const double* in_dot,
+                       double* out, double* out_dot, double gamma, double dtdh,
+                       const flo_policy* pol);
+
+int flo_sweep_trace_f64(const flo_grid* g, int dim, const double* in, double* out,
+                        double gamma, double dtdh, const flo_policy* pol, uint64_t* trace);
+
 /* Max over cells of max_d |u_d| + a (state/state_impl.hpp:167-178). */
 double flo_max_wavespeed_f64(const flo_grid* g, const double* in, double gamma);
 float  flo_max_wavespeed_f32(const flo_grid* g, const float* in, float gamma);

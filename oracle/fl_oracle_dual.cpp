@@ -62,25 +62,30 @@ inline double p_inf_now() { return flo_get_p_inf(); }
 
 #define flo_p_inf_ p_inf_now()
 #define T Dual
-#define SFX _dual
 #define SQRT(x) dual_sqrt(x)
 #define FABS(x) dual_fabs(x)
+// chi frozen: computed in double from the values, a constant here
+#define SFX _dual
 #include "fl_oracle_impl.inc"
-#undef T
 #undef SFX
+// chi differentiated: its ramp eta in dual numbers too
+#undef CHI_T
+#define CHI_T Dual
+#define SFX _dualchi
+#include "fl_oracle_impl.inc"
+#undef SFX
+#undef CHI_T
+#undef T
 #undef SQRT
 #undef FABS
 #undef flo_p_inf_
 
-}  // namespace
-
-extern "C" {
-
-/* One sweep of the FP64 oracle in dual numbers: out = sweep(in) and
- * out_dot = d sweep(in) [in_dot], with dtdh held constant. */
-int flo_sweep_dual(const flo_grid* g, int dim, const double* in, const double* in_dot,
-                   double* out, double* out_dot, double gamma, double dtdh,
-                   const flo_policy* pol) {
+// One sweep in dual numbers through SWEEP: out = sweep(in) and
+// out_dot = d sweep(in) [in_dot], with dtdh held constant.
+template <int (*SWEEP)(const flo_grid*, int, const Dual*, Dual*, Dual, Dual, const flo_policy*)>
+int sweep_dual_with(const flo_grid* g, int dim, const double* in, const double* in_dot,
+                    double* out, double* out_dot, double gamma, double dtdh,
+                    const flo_policy* pol) {
   if (!g || g->dims < 1 || g->dims > 3) return -1;
   int64_t cells = 1;
   for (int d = 0; d < g->dims; ++d) {
@@ -93,11 +98,33 @@ int flo_sweep_dual(const flo_grid* g, int dim, const double* in, const double* i
   Dual* b = (Dual*)malloc(sizeof(Dual) * n);
   if (!a || !b) { free(a); free(b); return -2; }
   for (size_t i = 0; i < n; ++i) { a[i] = Dual(in[i], in_dot[i]); b[i] = Dual(0.0); }
-  const int rc = sweep_impl_dual(g, dim, a, b, Dual(gamma), Dual(dtdh), pol);
+  const int rc = SWEEP(g, dim, a, b, Dual(gamma), Dual(dtdh), pol);
   for (size_t i = 0; i < n; ++i) { out[i] = b[i].v; out_dot[i] = b[i].d; }
   free(a);
   free(b);
   return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* One sweep of the FP64 oracle in dual numbers, the flattening coefficient
+ * frozen at its value (the map the adjoint transposes). */
+int flo_sweep_dual(const flo_grid* g, int dim, const double* in, const double* in_dot,
+                   double* out, double* out_dot, double gamma, double dtdh,
+                   const flo_policy* pol) {
+  return sweep_dual_with<sweep_impl_dual>(g, dim, in, in_dot, out, out_dot, gamma, dtdh, pol);
+}
+
+/* The same with the flattening coefficient differentiated through its ramp
+ * eta = 1 - (z - 0.75) / 0.1 (its clamps and min selections taken on the
+ * values): the derivative of the sweep as it is, where chi is active. */
+int flo_sweep_dual_chi(const flo_grid* g, int dim, const double* in, const double* in_dot,
+                       double* out, double* out_dot, double gamma, double dtdh,
+                       const flo_policy* pol) {
+  return sweep_dual_with<sweep_impl_dualchi>(g, dim, in, in_dot, out, out_dot, gamma, dtdh,
+                                             pol);
 }
 
 }  /* extern "C" */

@@ -116,8 +116,11 @@ def lib():
         L.flo_ls_velocity_f64.argtypes = [C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_int64, C.c_double, C.c_void_p]
         L.flo_ls_project_f64.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
+        L.flo_sweep_trace_f64.argtypes = [P(_Grid), C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_double, C.c_double, P(_Policy), C.c_void_p]
         L.flo_sweep_dual.argtypes = [P(_Grid), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_double, C.c_double, P(_Policy)]
+        L.flo_sweep_dual_chi.argtypes = L.flo_sweep_dual.argtypes
         L.flo_ls_weno_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double, C.c_void_p,
                                       C.c_void_p]
         L.flo_ls_godunov_f64.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_double,
@@ -261,28 +264,65 @@ def sweep(shape, dim, u, gamma, dtdh, **pol):
     return out
 
 
-def sweep_dual(shape, dim, u, du, gamma, dtdh, **pol):
+def sweep_dual(shape, dim, u, du, gamma, dtdh, chi_diff=False, **pol):
     """One FP64 sweep in forward-mode dual numbers: (sweep(u), derivative of
-    the sweep at u along du), with dtdh held constant, the branches of the
-    primal run and the flattening coefficient taken as a constant."""
+    the sweep at u along du), with dtdh held constant and the branches of
+    the primal run.  The flattening coefficient is taken as a constant (the
+    map the adjoint transposes), or with chi_diff differentiated through its
+    ramp (the derivative of the sweep itself where chi is active)."""
     g = _grid(shape)
     u = np.ascontiguousarray(u, dtype=np.float64)
     du = np.ascontiguousarray(du, dtype=np.float64)
     out, dout = np.empty_like(u), np.empty_like(u)
     p = _policy(**pol)
-    rc = lib().flo_sweep_dual(C.byref(g), dim, _ptr(u), _ptr(du), _ptr(out), _ptr(dout), gamma,
-                              dtdh, C.byref(p))
+    f = lib().flo_sweep_dual_chi if chi_diff else lib().flo_sweep_dual
+    rc = f(C.byref(g), dim, _ptr(u), _ptr(du), _ptr(out), _ptr(dout), gamma, dtdh, C.byref(p))
     if rc != 0:
         raise ValueError(f"dual sweep failed ({rc})")
     return out, dout
 
 
-def rollout_dual(shape, u, du, gamma, dtdh_seq, **pol):
-    """Steps with the given dt/dh sequence (sweeps x, y, z each step), in dual
-    numbers: returns the final state and its derivative along du."""
+def sweep_trace(shape, dim, u, gamma, dtdh, **pol):
+    """FP64 sweep with its branch trace: (out, trace), trace one uint64 hash
+    of the branch decisions per evolved cell and per face (fl_oracle.h)."""
+    g = _grid(shape)
+    p = _policy(**pol)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.empty_like(u)
+    n = shape[dim]
+    lines = int(np.prod(shape)) // n
+    trace = np.zeros(lines * (2 * n + 3), dtype=np.uint64)
+    rc = lib().flo_sweep_trace_f64(C.byref(g), dim, _ptr(u), _ptr(out), gamma, dtdh,
+                                   C.byref(p), _ptr(trace))
+    if rc != 0:
+        raise RuntimeError(f"flo_sweep_trace_f64 failed ({rc})")
+    return out, trace
+
+
+def rollout_trace(shape, u, gamma, dtdh_seq, **pol):
+    """Steps with the given dt/dh sequence (sweeps x, y, z each step):
+    (final state, one branch trace per sweep)."""
+    traces = []
     for dtdh in dtdh_seq:
         for dim in range(len(shape)):
-            u, du = sweep_dual(shape, dim, u, du, gamma, float(dtdh), **pol)
+            u, t = sweep_trace(shape, dim, u, gamma, float(dtdh), **pol)
+            traces.append(t)
+    return u, traces
+
+
+def branch_flips(traces_a, traces_b) -> int:
+    """Entries (evolved cells and faces over all sweeps) whose branch
+    decisions differ between two traced rollouts of the same shape."""
+    return int(sum(int(np.count_nonzero(a != b)) for a, b in zip(traces_a, traces_b)))
+
+
+def rollout_dual(shape, u, du, gamma, dtdh_seq, chi_diff=False, **pol):
+    """Steps with the given dt/dh sequence (sweeps x, y, z each step), in dual
+    numbers: returns the final state and its derivative along du (chi frozen,
+    or differentiated with chi_diff)."""
+    for dtdh in dtdh_seq:
+        for dim in range(len(shape)):
+            u, du = sweep_dual(shape, dim, u, du, gamma, float(dtdh), chi_diff=chi_diff, **pol)
     return u, du
 
 
