@@ -781,10 +781,12 @@ def adjoint_exactness(n=128, steps=40, directions=4, eps=1e-6):
     """The FP64 adjoint against an exact reference gradient at a size the CPU
     evaluates: per seeded direction, <adjoint gradient, v> against the
     directional derivative in forward-mode dual numbers through the oracle's
-    sweep (oracle/fl_oracle_dual.cpp; the same frozen branches, flattening
-    coefficient and time steps), and the central difference against that
-    exact value.  Where the adjoint matches the exact derivative to rounding,
-    a central difference that misses it is off by its own errors: limiter and
+    sweep (oracle/fl_oracle_dual.cpp; the same frozen branches and time
+    steps, the flattening coefficient differentiated through its ramp), the
+    central difference against that exact value, and the branch decisions
+    that differ between u + eps v and u - eps v (oracle.branch_flips).  Where
+    the adjoint matches the exact derivative to rounding, a central
+    difference that misses it is off by its own errors: limiter and
     wave-speed switches inside +-eps, and round-off in J(u+) - J(u-)."""
     import numpy as np
     import torch
@@ -804,7 +806,7 @@ def adjoint_exactness(n=128, steps=40, directions=4, eps=1e-6):
     z = np.zeros_like(r0)
     u0 = np.stack([r0, r0 / 0.4, z, z])
     t0 = time.perf_counter()
-    ad_err, fd_err, fd_chi_err, chi_terms, flips = [], [], [], [], []
+    ad_err, fd_chi_err, chi_terms, flips = [], [], [], []
 
     def directional(u, du):
         rho, e, mx, my = u
@@ -826,24 +828,24 @@ def adjoint_exactness(n=128, steps=40, directions=4, eps=1e-6):
             up = adj.forward(state_from_density(rho0.detach() + eps * v), 0.7, frozen_dtdh=dts)
             um = adj.forward(state_from_density(rho0.detach() - eps * v), 0.7, frozen_dtdh=dts)
             fd = objective_difference(up, um, p_target).item() / (2 * eps)
-            ad_err.append(abs(ad - exact) / abs(exact))
-            fd_err.append(abs(fd - exact) / abs(exact))
+            ad_err.append(abs(ad - exact_chi) / abs(exact_chi))
             fd_chi_err.append(abs(fd - exact_chi) / abs(exact_chi))
-            chi_terms.append(abs(exact_chi - exact) / abs(exact))
+            chi_terms.append(abs(exact_chi - exact) / abs(exact_chi))
             flips.append(oracle.branch_flips(tp, tm))
     del adj
     g3 = lambda xs: [float(f"{e:.3g}") for e in xs]
     return {"grid": f"{n}x{n}", "steps": steps, "reference": "oracle sweep in forward-mode "
-            "dual numbers (same frozen branches, chi and dt)", "cpu_s": time.perf_counter() - t0,
+            "dual numbers (the forward pass's branches and dt, chi differentiated through its "
+            "ramp)", "cpu_s": time.perf_counter() - t0,
             "adjoint_vs_exact_rel": g3(ad_err),
-            "central_difference_vs_exact_rel": g3(fd_err),
-            "central_difference_vs_exact_with_chi_rel": g3(fd_chi_err),
-            "chi_terms_rel": g3(chi_terms),
+            "central_difference_vs_exact_rel": g3(fd_chi_err),
             "branch_flips_between_u_plus_and_u_minus": flips,
-            "reading": "the adjoint equals the frozen-chi derivative to rounding; a central "
-                       "difference straddling no branch flip equals the chi-differentiated "
-                       "derivative (tests/test_branch_flips.py), and chi_terms_rel is what "
-                       "freezing chi leaves out",
+            "chi_terms_rel": g3(chi_terms),
+            "reading": "the adjoint equals the exact derivative to rounding; a central "
+                       "difference straddling no branch flip equals it too "
+                       "(tests/test_branch_flips.py), so the central differences' misses "
+                       "here come with flips; chi_terms_rel is the part of the derivative "
+                       "that chi's ramp contributes",
             "fd_eps": eps}
 
 

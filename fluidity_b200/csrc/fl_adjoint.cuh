@@ -5,8 +5,9 @@
 // forward function of the same name in fl_numerics.cuh, with every branch
 // taken as the forward pass takes it: the HLLC wave region and shock /
 // rarefaction choice, the max(0, p_pvrs) clamp and the minmod (van Leer)
-// selection are frozen at the forward values, and the flattening
-// coefficient chi is a frozen coefficient.  Functions are host + device so
+// selection are frozen at the forward values.  evolve_rev returns the
+// adjoint of the flattening coefficient chi; the sweep kernel carries it on
+// through chi's ramp (fl_adjoint_sweep.cuh).  Functions are host + device so
 // that tests/cpp/adjoint_fd.cpp can check them against finite differences on
 // the CPU.
 #pragma once
@@ -326,11 +327,13 @@ FL_HD void evolve_fwd(const Cons<T, D>& um, const Cons<T, D>& u, const Cons<T, D
 }
 
 // Reverse of evolve_fwd: given the adjoints of both evolved faces, the
-// adjoints of the cell and its two neighbours along the sweep.
+// adjoints of the cell and its two neighbours along the sweep, and in dchi
+// the adjoint of the flattening coefficient: sum_c 0.5 lim_c (bb_c - ab_c),
+// lim_c the limited slope that chi scales.
 template <typename T, int D>
 FL_HD void evolve_rev(const Cons<T, D>& um, const Cons<T, D>& u, const Cons<T, D>& up, T chi,
                       int d, T gm1, T dtdh, const Cons<T, D>& erb, const Cons<T, D>& elb,
-                      Cons<T, D>& dum, Cons<T, D>& du, Cons<T, D>& dup) {
+                      Cons<T, D>& dum, Cons<T, D>& du, Cons<T, D>& dup, T& dchi) {
   const T ch = chi * T(0.5);
   const T hd = T(0.5) * dtdh;
   Cons<T, D> a, b, ab, bb, fab, fbb;
@@ -351,9 +354,12 @@ FL_HD void evolve_rev(const Cons<T, D>& um, const Cons<T, D>& u, const Cons<T, D
   }
   flux_rev(a, derive(a, gm1), d, gm1, fab, ab);
   flux_rev(b, derive(b, gm1), d, gm1, fbb, bb);
+  T gchi = T(0);
 #pragma unroll
   for (int c = 0; c < D + 2; ++c) {
     du.v[c] += ab.v[c] + bb.v[c];
+    const T lim = choice[c] == 0 ? T(0) : (choice[c] == 1 ? u.v[c] - um.v[c] : up.v[c] - u.v[c]);
+    gchi += T(0.5) * lim * (bb.v[c] - ab.v[c]);
     const T limb = ch * (bb.v[c] - ab.v[c]);
     if (choice[c] == 1) {
       du.v[c] += limb;
@@ -363,6 +369,16 @@ FL_HD void evolve_rev(const Cons<T, D>& um, const Cons<T, D>& u, const Cons<T, D
       du.v[c] -= limb;
     }
   }
+  dchi = gchi;
+}
+
+// evolve_rev with the flattening coefficient's adjoint discarded.
+template <typename T, int D>
+FL_HD void evolve_rev(const Cons<T, D>& um, const Cons<T, D>& u, const Cons<T, D>& up, T chi,
+                      int d, T gm1, T dtdh, const Cons<T, D>& erb, const Cons<T, D>& elb,
+                      Cons<T, D>& dum, Cons<T, D>& du, Cons<T, D>& dup) {
+  T dchi;
+  evolve_rev(um, u, up, chi, d, gm1, dtdh, erb, elb, dum, du, dup, dchi);
 }
 
 }  // namespace fl

@@ -43,7 +43,21 @@ cudaError_t launch_adj_one(const AdjointParams& p, cudaStream_t st) {
   const dim3 grid((unsigned)((p.n[0] + G::T0 - 1) / G::T0),
                   (unsigned)((p.n[1] + G::T1 - 1) / G::T1), 1);
   k<<<grid, G::THREADS, G::smem_bytes, st>>>(p);
-  return cudaGetLastError();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (p.chi_gz != nullptr && p.flatten && !p.basic) {
+    // the chi terms, gathered per cell from the records the sweep left
+    const int64_t cells = p.n[0] * (D >= 2 ? p.n[1] : 1);
+    const int64_t blocks = (cells + 255) / 256;
+    adj_chi_gather_kernel<T, D, S><<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), 256, 0,
+                                     st>>>(static_cast<const T*>(p.u),
+                                           static_cast<const T*>(p.chi_gz), p.chi_epoch_of,
+                                           p.chi_sel, p.chi_flag, p.chi_epoch,
+                                           static_cast<T*>(p.lam_in), p.pitch, p.n[0], p.n[1],
+                                           (T)p.gamma - T(1));
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 template <typename T, int FLUX>
@@ -90,6 +104,31 @@ int check_adj_material(const fl_material* m) {
   if (!(m->p_inf >= 0.0) || m->p_inf > DBL_MAX)
     return set_error(kEInval, "p_inf must be finite and >= 0");
   return kOk;
+}
+
+// chi records for the widest sweep of the grid: (n_S + 2) * lines.
+int64_t chi_record_count(const fl_grid* g) {
+  if (g->dims == 1) return g->n[0] + 2;
+  return std::max((g->n[0] + 2) * g->n[1], (g->n[1] + 2) * g->n[0]);
+}
+
+// Layout of count records: values (elem bytes each), epochs (4), selection
+// bytes (1), then the two flag words, each part 16-byte aligned.
+size_t chi_record_bytes(int64_t count, int elem) {
+  auto al = [](size_t b) { return (b + 15) / 16 * 16; };
+  return al((size_t)count * elem) + al((size_t)count * 4) + al((size_t)count) + 16;
+}
+
+void set_chi_records(AdjointParams& p, char* base, int64_t count, int elem, unsigned int epoch) {
+  auto al = [](size_t b) { return (b + 15) / 16 * 16; };
+  const size_t o1 = al((size_t)count * elem);
+  const size_t o2 = o1 + al((size_t)count * 4);
+  const size_t o3 = o2 + al((size_t)count);
+  p.chi_gz = base;
+  p.chi_epoch_of = reinterpret_cast<unsigned int*>(base + o1);
+  p.chi_sel = reinterpret_cast<unsigned char*>(base + o2);
+  p.chi_flag = reinterpret_cast<unsigned int*>(base + o3);
+  p.chi_epoch = epoch;
 }
 
 AdjointParams make_adj_params(const fl_grid* g, uint32_t policy, double gamma, double pinf,
@@ -179,6 +218,9 @@ struct fl_adj {
   char* ckpt = nullptr;     // (nsteps / interval + 1) states
   char* seg = nullptr;      // dims * interval states
   char* work = nullptr;     // 4 states: forward ping-pong, adjoint ping-pong
+  char* chi_rec = nullptr;  // chi records of the widest sweep (chi_record_bytes)
+  int64_t chi_count = 0;
+  unsigned int chi_epoch = 0;  // adjoint sweeps run: names the records of each
   StepControl* ctrl = nullptr;
   double* d_dtdh = nullptr;
   std::vector<double> dtdh;
@@ -220,8 +262,24 @@ int fl_adjoint_sweep_mat(const fl_grid* grid, int dim, const void* u_in,
   p.u = u_in;
   p.lam_out = lambda_out;
   p.lam_in = lambda_in;
-  cudaError_t e = launch_adj(p, policy & 1u, (int)((policy >> 1) & 3u), grid->dims, dim,
-                             static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaSuccess;
+  void* rec = nullptr;
+  if (p.flatten && !p.basic) {
+    // the chi terms need records for this call, epochs and flags at 0
+    const int64_t count = chi_record_count(grid);
+    const int elem = (policy & 1u) ? 4 : 8;
+    const size_t bytes = chi_record_bytes(count, elem);
+    e = cudaMallocAsync(&rec, bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(rec, 0, bytes, st);
+    set_chi_records(p, static_cast<char*>(rec), count, elem, 1u);
+  }
+  if (e == cudaSuccess)
+    e = launch_adj(p, policy & 1u, (int)((policy >> 1) & 3u), grid->dims, dim, st);
+  if (rec != nullptr) {
+    const cudaError_t ef = cudaFreeAsync(rec, st);
+    if (e == cudaSuccess) e = ef;
+  }
   if (e != cudaSuccess) return set_error(kECuda, "fl_adjoint_sweep: %s", cudaGetErrorString(e));
   return kOk;
 }
@@ -255,6 +313,10 @@ int fl_adj_create(fl_adj** out, const fl_grid* grid, double gamma, uint32_t poli
   cudaError_t e = cudaMalloc(&a->ckpt, a->state_bytes * nck);
   if (e == cudaSuccess) e = cudaMalloc(&a->seg, a->state_bytes * grid->dims * interval);
   if (e == cudaSuccess) e = cudaMalloc(&a->work, a->state_bytes * 4);
+  a->chi_count = chi_record_count(grid);
+  const size_t rec_bytes = chi_record_bytes(a->chi_count, (policy & 1u) ? 4 : 8);
+  if (e == cudaSuccess) e = cudaMalloc(&a->chi_rec, rec_bytes);
+  if (e == cudaSuccess) e = cudaMemset(a->chi_rec, 0, rec_bytes);   // epochs and flags 0
   if (e == cudaSuccess) e = cudaMalloc(&a->ctrl, sizeof(StepControl));
   if (e == cudaSuccess) e = cudaMemset(a->ctrl, 0, sizeof(StepControl));  // strip counters at 0
   if (e == cudaSuccess) e = cudaMalloc(&a->d_dtdh, sizeof(double) * nsteps);
@@ -282,6 +344,7 @@ int fl_adj_destroy(fl_adj* a) {
   cudaFree(a->ckpt);
   cudaFree(a->seg);
   cudaFree(a->work);
+  cudaFree(a->chi_rec);
   cudaFree(a->ctrl);
   cudaFree(a->d_dtdh);
   delete a;
@@ -431,6 +494,8 @@ int fl_adj_backward(fl_adj* a, const void* lambda_final, void* lambda_0, void* s
         p.u = state_at(a->seg, sb, (k - k0) * D + d);
         p.lam_out = la;
         p.lam_in = lb;
+        if (++a->chi_epoch == 0u) a->chi_epoch = 1u;   // 0 marks records never written
+        set_chi_records(p, a->chi_rec, a->chi_count, f32 ? 4 : 8, a->chi_epoch);
         e = launch_adj(p, f32, flux, D, d, st);
         void* t = la;
         la = lb;

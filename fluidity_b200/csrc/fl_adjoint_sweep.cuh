@@ -9,11 +9,20 @@
 //   lam_i      = lam'_i + dUp_{i-1} + dU_i + dUm_{i+1}
 // plus, at the two ends of the domain, the adjoints that reach ghost cells
 // folded back onto the cells they mirror (the normal momentum negated at a
-// reflective end).  chi and the wave/limiter branches are frozen (see
-// fl_adjoint.cuh), so lines along the sweep are independent; chi's value
-// still needs the cross-dimension neighbours.  Tile: T_S cells along the
-// sweep, halo 5 along it (the forward faces of evolve cells [-2, T_S+1]),
-// 3 across.
+// reflective end).  The wave/limiter branches are frozen (see
+// fl_adjoint.cuh), so lines along the sweep are independent, except for
+// the flattening coefficient chi.  chi_v(e) = min over dimensions of
+// min(chi_d(e), chi_d(e + sign e_d)) is differentiated through the one
+// chi_d(c*) the minimum selects, where that one lies on its ramp
+// eta = 1 - (z - 0.75) / 0.1, z = |p(c*+1) - p(c*-1)| / |p(c*+2) - p(c*-2)|
+// along d (muscl_reconstructor.hpp:59-111); its clamps, the flattening test
+// and the selection are frozen.  Those four pressures can lie on other
+// lines, so each evolve cell leaves a record (which chi_d it selected, and
+// dL/dchi dchi/dz), and a second kernel gathers per cell, in a fixed order,
+// the records whose stencils read its pressure, and adds them to lam_in
+// through dp/dU: no atomics, the same result on every run.  Tile: T_S cells
+// along the sweep, halo 5 along it (the forward faces of evolve cells
+// [-2, T_S+1]), 3 across.
 #pragma once
 
 #include <cfloat>
@@ -37,7 +46,25 @@ struct AdjointParams {
   int flatten;
   int basic;
   uint32_t reflect;
+  // nullable: the chi records, one per evolve cell of every line
+  // ((n_S + 2) * lines, evolve cells -1 .. n_S along the sweep): chi_gz the
+  // sweep's dtype, chi_epoch the sweep that wrote the record, chi_sel the
+  // selection byte; a record counts only in the sweep chi_epoch names.
+  // chi_flag[chi_epoch & 1] is set when the sweep wrote any record, and the
+  // gather clears the other word for the next sweep.  Without records chi
+  // is frozen.
+  void* chi_gz;
+  unsigned int* chi_epoch_of;
+  unsigned char* chi_sel;
+  unsigned int* chi_flag;
+  unsigned int chi_epoch;
 };
+
+// Index of evolve cell (along the sweep eS in [-1, nS], across eA) in the
+// chi records.
+__host__ __device__ __forceinline__ int64_t chi_rec(int64_t eS, int64_t eA, int64_t nS) {
+  return eA * (nS + 2) + (eS + 1);
+}
 
 template <int D, int S>
 struct AdjTile {
@@ -77,11 +104,114 @@ struct AdjGeom {
       + E                                   // chi_v of evolve cells
       + 4 * NC * E                          // er, el, er_b, el_b
       + NC * E;                             // lam_out on evolve cells
-  static constexpr size_t smem_bytes = sizeof(T) * smem_elems + 64;
+  // plus one byte per evolve cell: which chi_d the minimum selected
+  static constexpr size_t smem_bytes = sizeof(T) * smem_elems + E + 64;
   __host__ __device__ static constexpr int rstride(int d) { return d == 0 ? 1 : R0; }
   __host__ __device__ static constexpr int estride(int d) { return d == 0 ? 1 : E0; }
   __host__ __device__ static constexpr int tile(int d) { return d == 0 ? T0 : T1; }
 };
+
+// dchi/dz on the ramp eta = 1 - (z - 0.75) / (0.85 - 0.75)
+template <typename T>
+__host__ __device__ constexpr T chi_dz() { return T(-1.0 / (0.85 - 0.75)); }
+
+// Pressure of the state at global position (x0, x1), mirrored into the
+// domain (a reflective flip changes no pressure).
+template <typename T, int D>
+__device__ __forceinline__ T adj_pressure_at(const T* u_in, int64_t pitch, int64_t n0, int64_t n1,
+                                             int64_t x0, int64_t x1, T gm1) {
+  bool f;
+  const int64_t g0 = mirror_index(x0, n0, f);
+  const int64_t g1 = (D >= 2) ? mirror_index(x1, n1, f) : 0;
+  const int64_t gi = g1 * n0 + g0;
+  Cons<T, D> u;
+#pragma unroll
+  for (int c = 0; c < D + 2; ++c) u.v[c] = u_in[c * pitch + gi];
+  return derive(u, gm1).p;
+}
+
+// Positions that mirror onto cell c of an extent-n dimension within 4
+// cells of the domain: c, and its images -1 - c and 2n - 1 - c.
+__device__ __forceinline__ int chi_images(int64_t c, int64_t n, int64_t* x) {
+  int k = 0;
+  x[k++] = c;
+  if (-1 - c >= -4) x[k++] = -1 - c;
+  if (2 * n - 1 - c <= n + 3) x[k++] = 2 * n - 1 - c;
+  return k;
+}
+
+// The chi terms: per cell c, the pressure adjoint gathered from every evolve
+// cell whose selected chi_d(c*) reads a position x that mirrors onto c
+// (x = c* + o e_d, o = +-1, +-2), then lam_in(c) += lam_p dp/dU(c).
+template <typename T, int D, int S>
+__global__ void adj_chi_gather_kernel(const T* __restrict__ u_in, const T* __restrict__ gz,
+                                      const unsigned int* __restrict__ epoch_of,
+                                      const unsigned char* __restrict__ sel,
+                                      unsigned int* __restrict__ flag, unsigned int epoch,
+                                      T* __restrict__ lam_in, int64_t pitch, int64_t n0,
+                                      int64_t n1, T gm1) {
+  // the next sweep's flag word is free: this sweep's main kernel is done
+  // with it and the next one has not started
+  if (blockIdx.x == 0 && threadIdx.x == 0) flag[(epoch + 1u) & 1u] = 0u;
+  if (*(volatile unsigned int*)(flag + (epoch & 1u)) == 0u) return;  // no chi terms
+  const int64_t nS = (S == 0) ? n0 : n1;
+  const int64_t nA = (D >= 2) ? ((S == 0) ? n1 : n0) : 1;
+  const int64_t cells = n0 * ((D >= 2) ? n1 : 1);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c0 = i % n0, c1 = (D >= 2) ? i / n0 : 0;
+    int64_t xs0[3], xs1[3];
+    const int k0 = chi_images(c0, n0, xs0);
+    int k1 = 1;
+    xs1[0] = 0;
+    if (D >= 2) k1 = chi_images(c1, n1, xs1);
+    T lp = T(0);
+    for (int ia = 0; ia < k0; ++ia)
+      for (int ib = 0; ib < k1; ++ib)
+        for (int d = 0; d < D; ++d) {
+          const int64_t s0 = (d == 0) ? 1 : 0, s1 = (d == 1) ? 1 : 0;
+          for (int oi = 0; oi < 4; ++oi) {
+            const int o = (oi == 0) ? 1 : (oi == 1) ? -1 : (oi == 2) ? 2 : -2;
+            const int64_t q0 = xs0[ia] - o * s0, q1 = xs1[ib] - o * s1;   // c*
+            for (int si = 0; si < 3; ++si) {
+              const int side = si - 1;
+              const int64_t e0 = q0 - side * s0, e1 = q1 - side * s1;
+              const int64_t eS = (S == 0) ? e0 : e1, eA = (S == 0) ? e1 : e0;
+              if (eS < -1 || eS > nS || eA < 0 || eA >= nA) continue;
+              const int64_t r = chi_rec(eS, eA, nS);
+              if (epoch_of[r] != epoch || sel[r] != d * 3 + si) continue;
+              const T pp1 = adj_pressure_at<T, D>(u_in, pitch, n0, n1, q0 + s0, q1 + s1, gm1);
+              const T pm1 = adj_pressure_at<T, D>(u_in, pitch, n0, n1, q0 - s0, q1 - s1, gm1);
+              const T pp2 = adj_pressure_at<T, D>(u_in, pitch, n0, n1, q0 + 2 * s0,
+                                                  q1 + 2 * s1, gm1);
+              const T pm2 = adj_pressure_at<T, D>(u_in, pitch, n0, n1, q0 - 2 * s0,
+                                                  q1 - 2 * s1, gm1);
+              const T a = pp1 - pm1, b = pp2 - pm2;
+              const T ab = fl_abs<T>(b);
+              const T sa = (a < T(0)) ? T(-1) : T(1), sb = (b < T(0)) ? T(-1) : T(1);
+              T dzdp;  // dz / dp(x), z = |a| / |b|
+              if (o == 1) dzdp = sa / ab;
+              else if (o == -1) dzdp = -sa / ab;
+              else if (o == 2) dzdp = -(fl_abs<T>(a) / ab) * sb / ab;
+              else dzdp = (fl_abs<T>(a) / ab) * sb / ab;
+              lp += gz[r] * dzdp;
+            }
+          }
+        }
+    if (lp == T(0)) continue;
+    Cons<T, D> u, ub;
+#pragma unroll
+    for (int c = 0; c < D + 2; ++c) {
+      u.v[c] = u_in[c * pitch + i];
+      ub.v[c] = T(0);
+    }
+    DerivedBar<T, D> qb = zero_bar<T, D>();
+    qb.p = lp;
+    derive_rev(u, derive(u, gm1), gm1, qb, ub);
+#pragma unroll
+    for (int c = 0; c < D + 2; ++c) lam_in[c * pitch + i] += ub.v[c];
+  }
+}
 
 template <typename T, int D, int S, int FLUX>
 __global__ void __launch_bounds__(AdjGeom<T, D, S>::THREADS, AdjGeom<T, D, S>::MIN_CTAS)
@@ -110,6 +240,10 @@ adjoint_sweep_kernel(AdjointParams p) {
   T* sDm = sER;                   // stages E-F: er, el and P/V/chi are dead
   T* sD0 = sEL;
   T* sDp = sP;
+  // chi selection per evolve cell: 255 = no derivative, else
+  // d * 3 + (side + 1) with chi_d taken at e + side e_d
+  unsigned char* sSel = reinterpret_cast<unsigned char*>(sLam + NC * G::E);
+  const bool chi_diff = flatten && p.chi_gz != nullptr;
 
   const T* __restrict__ u_in = static_cast<const T*>(p.u);
   const T* __restrict__ lo = static_cast<const T*>(p.lam_out);
@@ -192,6 +326,7 @@ adjoint_sweep_kernel(AdjointParams p) {
       up.v[c] = sU[c * G::R + q + SS];
     }
     T chi_v = T(1);
+    int sel = 255;
     if (flatten) {
       chi_v = (sizeof(T) == 8) ? (T)DBL_MAX : (T)FLT_MAX;
 #pragma unroll
@@ -200,10 +335,20 @@ adjoint_sweep_kernel(AdjointParams p) {
         const T diff = sP[q + st] - sP[q - st];
         const int sign = (T(0) < diff) - (diff < T(0));
         const T* cd = sChi + d * G::R;
-        chi_v = std_min(chi_v, std_min(cd[q], cd[q + sign * st]));
+        // std_min(a, b) keeps a unless b < a: the same choice recorded
+        const T c0 = cd[q], c1 = cd[q + sign * st];
+        const bool nb = c1 < c0;
+        const T m = nb ? c1 : c0;
+        if (m < chi_v) {
+          chi_v = m;
+          sel = d * 3 + (nb ? sign : 0) + 1;
+        }
       }
+      // on the ramp only: the clamps and an unflattened 1 carry no derivative
+      if (!(chi_v > T(0) && chi_v < T(1))) sel = 255;
     }
     sCv[e] = chi_v;
+    sSel[e] = (unsigned char)sel;
     if (muscl) {
       evolve_fwd(um, u, up, chi_v, S, gm1, dtdh, er, el);
     } else {
@@ -279,7 +424,29 @@ adjoint_sweep_kernel(AdjointParams p) {
         elb.v[c] = sELb[c * G::E + e];
       }
       if (muscl) {
-        evolve_rev(um, u, up, sCv[e], S, gm1, dtdh, erb, elb, dm, d0, dp);
+        T dchi;
+        evolve_rev(um, u, up, sCv[e], S, gm1, dtdh, erb, elb, dm, d0, dp, dchi);
+        if (chi_diff) {
+          // records of the evolve cells owned here: the tile's cells, and
+          // the ghost evolve cells -1 and nS at the domain's ends (nS in the
+          // tile of cell nS - 1 only); -2 and nS + 1 feed ghost faces only
+          const int es = (S == 0) ? e0 : e1;
+          const int64_t ge0 = o0 + e0 - (S == 0 ? 2 : 0);
+          const int64_t ge1 = o1 + e1 - (S == 1 ? 2 : 0);
+          const int64_t gs = (S == 0) ? ge0 : ge1;
+          const int64_t ga = (S == 0) ? ge1 : ge0;
+          const int64_t na = (D >= 2) ? ((S == 0) ? n1 : n0) : 1;
+          const bool own = ((es >= 2 && es < 2 + G::tile(S) && gs < nS) || gs == -1 ||
+                            (gs == nS && oS <= nS - 1 && nS - 1 < oS + G::tile(S))) &&
+                           ga < na;
+          if (own && sSel[e] != 255 && dchi != T(0)) {
+            const int64_t r = chi_rec(gs, ga, nS);
+            static_cast<T*>(p.chi_gz)[r] = dchi * chi_dz<T>();
+            p.chi_sel[r] = sSel[e];
+            p.chi_epoch_of[r] = p.chi_epoch;
+            p.chi_flag[p.chi_epoch & 1u] = 1u;
+          }
+        }
       } else {
 #pragma unroll
         for (int c = 0; c < NC; ++c) d0.v[c] = erb.v[c] + elb.v[c];

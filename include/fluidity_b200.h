@@ -399,8 +399,11 @@ int fl_batch_tuning(const fl_batch* batch, int32_t* out, int32_t n);
  * No reference counterpart (the reference has no differentiation).  Reverse
  * mode of the sweep with the HLLC wave region, shock/rarefaction choice,
  * pressure clamp and limiter (minmod) selection frozen at the forward pass,
- * the flattening coefficient chi frozen as a coefficient, and the CFL time
- * step frozen.  1-D and 2-D grids, HLLC or FORCE, van Leer limiter. */
+ * the flattening coefficient chi differentiated through its ramp
+ * eta = 1 - (z - 0.75) / 0.1 (its clamps, test and min selection frozen),
+ * and the CFL time step frozen.  1-D and 2-D grids, HLLC or FORCE, van Leer
+ * limiter.  With flattening on, fl_adjoint_sweep takes its chi records
+ * from the stream-ordered pool for the call; fl_adj_create allocates them. */
 
 /* lambda_in = (d sweep / d u_in)^T lambda_out for one dimensional sweep with
  * the given dtdh (u_in: the sweep's input state). */

@@ -58,6 +58,7 @@ static C2 rs_which(int which, const C2& l, const C2& r, int d, double dtdh) {
 
 int main() {
   double worst_flux = 0, worst_hllc = 0, worst_force = 0, worst_evolve = 0, worst_stiff = 0;
+  double worst_chi = 0;
   int regions[4] = {0, 0, 0, 0};
   for (int trial = 0; trial < 4000; ++trial) {
     const C2 a = rand_state(), b = rand_state(), c3 = rand_state();
@@ -126,7 +127,7 @@ int main() {
         worst_force = std::fmax(worst_force, err);
       }
     }
-    // evolve: chi frozen
+    // evolve (chi held), and the adjoint of chi itself
     {
       const double chi = (trial % 3 == 0) ? 1.0 : U(0, 1);
       C2 erp, elp, erm, elm, eb, lb;
@@ -146,8 +147,25 @@ int main() {
       zero(dum);
       zero(du);
       zero(dup);
-      evolve_rev(a, b, c3, chi, d, gm1, dtdh, eb, lb, dum, du, dup);
+      double dchi = 0.0;
+      evolve_rev(a, b, c3, chi, d, gm1, dtdh, eb, lb, dum, du, dup, dchi);
       const double ad = dot(dum, dl) + dot(du, dm) + dot(dup, dr);
+      // the adjoint of chi against a central difference in chi alone
+      {
+        const double he = 1e-6;
+        C2 er2p, el2p, er2m, el2m;
+        evolve_fwd(a, b, c3, chi + he, d, gm1, dtdh, er2p, el2p);
+        evolve_fwd(a, b, c3, chi - he, d, gm1, dtdh, er2m, el2m);
+        double fdc = 0, scc = 0;
+        for (int c = 0; c < 4; ++c) {
+          const double t = eb.v[c] * (er2p.v[c] - er2m.v[c]) / (2 * he) +
+                           lb.v[c] * (el2p.v[c] - el2m.v[c]) / (2 * he);
+          fdc += t;
+          scc += std::fabs(t);
+        }
+        worst_chi = std::fmax(worst_chi, std::fabs(fdc - dchi) / std::fmax(std::fabs(dchi),
+                                                                          std::fmax(scc, 1e-30)));
+      }
       const double err = std::fabs(fd - ad) / std::fmax(std::fabs(ad), sc);
       // minmod selection flips are piecewise: skip draws whose selection differs across +-eps
       bool flip = false;
@@ -164,9 +182,10 @@ int main() {
     }
     (void)regions;
   }
-  std::printf("flux %.3e hllc %.3e stiff hllc %.3e force %.3e evolve %.3e\n", worst_flux,
-              worst_hllc, worst_stiff, worst_force, worst_evolve);
+  std::printf("flux %.3e hllc %.3e stiff hllc %.3e force %.3e evolve %.3e chi %.3e\n",
+              worst_flux, worst_hllc, worst_stiff, worst_force, worst_evolve, worst_chi);
   const double tol = 1e-5;
   return (worst_flux < tol && worst_hllc < tol && worst_stiff < tol && worst_force < tol &&
+          worst_chi < tol &&
           worst_evolve < tol) ? 0 : 1;
 }

@@ -181,10 +181,10 @@ def test_adjoint_gradient_muscl_matches_finite_differences(cuda):
     assert max(errs) < 1e-3
 
 
-def test_adjoint_gradient_with_frozen_flattening(cuda):
-    """With flattening the adjoint holds chi frozen at its forward value, so
-    it differs from FD also through chi's own sensitivity: the mismatch is
-    reported and must stay small on this field."""
+def test_adjoint_gradient_with_flattening(cuda):
+    """With flattening on (chi differentiated through its ramp), against
+    central differences on a smooth field: reported, and held to the FD
+    noise and limiter-switch level of this field."""
     import torch
     rho0, adj, p_target, J0, grad = _gradient_case((48, 48), nsteps=8, interval=3, smooth=True)
     assert J0 > 0 and torch.norm(grad).item() > 0
@@ -364,11 +364,12 @@ def test_adjoint_set_material_drops_the_forward_pass(cuda):
     assert adj.lib.fl_adj_set_material(adj.handle, C.byref(bad)) != 0
 
 
-def _dual_directional(rho0, dts, p_target, v, gamma=1.4, **pol):
+def _dual_directional(rho0, dts, p_target, v, gamma=1.4, chi_diff=True, **pol):
     """J'(rho0)[v] from the oracle's sweep in forward-mode dual numbers
     (oracle/fl_oracle_dual.cpp) over the frozen time steps: the exact
-    derivative of the discrete map whose branches, flattening coefficient
-    and dt are those of the forward pass -- the map the adjoint transposes."""
+    derivative of the discrete map whose branches and dt are those of the
+    forward pass, with the flattening coefficient differentiated through its
+    ramp (chi_diff; frozen otherwise) -- the map the adjoint transposes."""
     import numpy as np
     from oracle import oracle
     n = int(round(rho0.size ** 0.5))
@@ -376,7 +377,7 @@ def _dual_directional(rho0, dts, p_target, v, gamma=1.4, **pol):
     z = np.zeros_like(rho0)
     u0 = np.stack([rho0, rho0 / (gamma - 1.0), z, z])     # state_from_density, p = rho
     du0 = np.stack([v, v / (gamma - 1.0), z, z])
-    u, du = oracle.rollout_dual(shape, u0, du0, gamma, dts, **pol)
+    u, du = oracle.rollout_dual(shape, u0, du0, gamma, dts, chi_diff=chi_diff, **pol)
     rho, e, mx, my = u
     drho, de, dmx, dmy = du
     ke = 0.5 * (mx * mx + my * my) / rho
@@ -410,12 +411,14 @@ def test_adjoint_gradient_matches_fp64_reference_gradient(cuda, oracle, case):
     """The adjoint's gradient against an independent FP64 reference gradient:
     directional derivatives along seeded directions computed in forward-mode
     dual numbers through the CPU oracle's own sweep, with the forward pass's
-    time steps.  Both are exact derivatives of the same frozen-branch map
-    (flattening coefficient frozen in both), so they agree to rounding:
-    1e-12 relative per direction, where finite differences stop at their
-    noise floor and at every limiter switch inside +-eps.  The ramp case has
-    the flattening coefficient active (checked: the oracle's rollouts with
-    and without flattening differ)."""
+    time steps and the flattening coefficient differentiated through its
+    ramp.  Both are exact derivatives of the same frozen-branch map, so they
+    agree to rounding: 1e-12 relative per direction, where finite
+    differences stop at their noise floor and at every limiter switch inside
+    +-eps.  The ramp case has the flattening coefficient active and on its
+    ramp: the oracle's rollouts with and without flattening differ, and the
+    derivative with chi frozen differs from the one with chi differentiated,
+    so the chi terms are part of what is checked."""
     import numpy as np
     import torch
     from fluidity_b200.adjoint import random_directions
@@ -437,9 +440,15 @@ def test_adjoint_gradient_matches_fp64_reference_gradient(cuda, oracle, case):
     r0 = rho0.detach().cpu().numpy()
     pt = p_target.cpu().numpy()
     errs = []
+    chi_terms = []
     for v in random_directions(r0.size, 4, seed=11):
         ref = _dual_directional(r0, dts, pt, v.cpu().numpy(), flatten=flatten)
         ad = torch.dot(grad, v).item()
         errs.append(abs(ad - ref) / abs(ref))
-    print("adjoint vs dual-number reference gradient:", ["%.2e" % e for e in errs])
+        frozen = _dual_directional(r0, dts, pt, v.cpu().numpy(), chi_diff=False, flatten=flatten)
+        chi_terms.append(abs(frozen - ref) / abs(ref))
+    print("adjoint vs dual-number reference gradient:", ["%.2e" % e for e in errs],
+          "; chi terms:", ["%.2e" % e for e in chi_terms])
     assert max(errs) < 1e-12
+    if case == "ramp_flatten_active":
+        assert max(chi_terms) > 1e-6, "chi never on its ramp"
