@@ -861,6 +861,53 @@ int fl_sim_sweep(fl_sim* sim, int dim, void* stream) {
   return kOk;
 }
 
+}  // extern "C"
+
+namespace fl {
+
+int sim_sweep_part(fl_sim* sim, int dim, int64_t row_lo, int64_t row_hi, unsigned int* counters,
+                   int slot, int last_part, void* stream) {
+  if (sim == nullptr || sim->a == nullptr) return fail(kEInval, "fl_sim_begin not called");
+  if (sim->grid.dims != 2) return fail(kEInval, "sweep parts are 2-D");
+  if (!sim->external) return fail(kEInval, "sweep parts need the external reduction");
+  if (dim != sim->cursor) return fail(kEInval, "sweep %d expected, %d given", sim->cursor, dim);
+  if (row_lo < 0 || row_hi > sim->grid.n[1])
+    return fail(kEInval, "rows [%lld, %lld) outside the grid", (long long)row_lo,
+                (long long)row_hi);
+  if (row_lo < row_hi) {
+    void* si = (dim & 1) ? sim->b : sim->a;
+    void* so = (dim & 1) ? sim->a : sim->b;
+    SweepParams p = make_params(&sim->grid, sim->pol, sim->gamma, sim->pinf, 0.0, sim->boundary);
+    p.ctrl = sim->ctrl;
+    p.ws_lo = sim->own_lo;
+    p.ws_hi = sim->own_hi;
+    p.walk_next = counters;
+    p.walk_slot = slot;
+    p.status = &sim->ctrl->status;
+    p.in = si;
+    p.out = so;
+    p.row_lo = row_lo;
+    p.row_hi = row_hi;
+    p.ws_accum = (dim == 1) ? (sim->external ? sim->ws_word : &sim->ctrl->ws_bits) : nullptr;
+    p.finalize = 0;
+    cudaError_t e = launch_sweep(p, sim->pol, 2, dim, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "fl_slab sweep");
+  }
+  if (last_part) {
+    if (dim == 1) {
+      sim->cursor = 0;
+      sim->enqueued += 1;
+    } else {
+      sim->cursor = dim + 1;
+    }
+  }
+  return kOk;
+}
+
+}  // namespace fl
+
+extern "C" {
+
 int fl_sim_finalize(fl_sim* sim, int advance, void* stream) {
   if (sim == nullptr) return fail(kEInval, "sim is NULL");
   finalize_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(

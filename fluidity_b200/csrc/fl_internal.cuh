@@ -62,12 +62,32 @@ struct SweepParams {
   // nullable: a kernel whose bounded wait on its own copies gave up writes
   // kETimeout here (and stops the loop through ctrl->done when ctrl is set)
   int* status;
+  // 2-D only: compute the output rows [row_lo, row_hi) of the slowest
+  // dimension only (reads reach beyond as usual); every row when
+  // row_hi <= row_lo.  Taken by the register walk and, for the y sweep, the
+  // staged walk.
+  int64_t row_lo, row_hi;
   // 2-D only, 1: the sweep of the layout-alternating loop.  `in` holds the
   // state with the sweep dimension slowest (x sweep: y fastest; y sweep:
   // x fastest) and `out` receives it transposed (x sweep: x fastest; y
   // sweep: y fastest).  Both layouts keep the planes `pitch` apart.
   int transposed;
 };
+
+}  // namespace fl
+
+typedef struct fl_sim fl_sim;
+
+namespace fl {
+
+// One part of sweep `dim` of the current step of a 2-D fl_sim loop in its
+// external-reduction mode: output rows [row_lo, row_hi) of the slowest
+// dimension (nothing is launched for an empty range), strips taken from the
+// two counters `counters` (slot `slot`; nullptr: the static grid).  The
+// part with last_part set ends the sweep (the loop's cursor moves on).
+// Defined in fl_api.cu; the slab step splits each sweep into parts.
+int sim_sweep_part(fl_sim* sim, int dim, int64_t row_lo, int64_t row_hi, unsigned int* counters,
+                   int slot, int last_part, void* stream);
 
 // Tensor map of one SoA state buffer for the TMA-staged sweeps: a 3-D
 // tensor (x, y, component plane) of n0 x n1 x planes elements with rows n0

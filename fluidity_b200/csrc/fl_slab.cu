@@ -40,6 +40,7 @@ namespace {
 constexpr int kRowsX = 3;           // ghost rows the x sweep reads
 constexpr int kRowsY = 4;           // ghost rows the y sweep reads
 constexpr int kMaxLocal = 16;       // slabs of one in-process group
+constexpr int kParts = 6;           // sweep parts per step (3 per sweep)
 
 // ---- NCCL, resolved at run time ---------------------------------------------
 struct NcclApi {
@@ -115,6 +116,16 @@ struct fl_slab {
   // state buffers of the run in progress
   char* a = nullptr;
   char* b = nullptr;
+  // the overlap: exchanges and collectives on a stream of the slab's own,
+  // joined to the caller's stream by events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // strip counters, a pair per sweep part (interior, lower edge, upper edge
+  // of the x and the y sweep); each part takes slot `parity` and clears the
+  // other, and parity flips every step
+  unsigned int* counters = nullptr;
+  int parity = 0;
+  bool counters_dirty = false;
 };
 
 namespace {
@@ -151,10 +162,16 @@ int make_slab(fl_slab** out, const fl_grid* grid, double gamma, uint32_t policy,
     if (e != cudaSuccess) rc = fl::set_error(FL_ENOMEM, "fl_slab: %s", cudaGetErrorString(e));
   }
   if (rc == FL_OK) rc = fl_sim_set_ws_word(s->sim, s->word);
+  if (rc == FL_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i)
+      e = cudaEventCreateWithFlags(&s->ev[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&s->counters, kParts * 2 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(s->counters, 0, kParts * 2 * sizeof(unsigned int));
+    if (e != cudaSuccess) rc = fl::set_error(FL_ECUDA, "fl_slab: %s", cudaGetErrorString(e));
+  }
   if (rc != FL_OK) {
-    if (s->word) cudaFree(s->word);
-    if (s->sim) fl_sim_destroy(s->sim);
-    delete s;
+    fl_slab_destroy(s);
     return rc;
   }
   *out = s;
@@ -367,14 +384,78 @@ int fl_slab_steps(fl_slab* const* slabs, int count, int64_t nsteps, void* stream
   for (int i = 0; i < count; ++i)
     if (slabs[i]->a == nullptr) return fl::set_error(FL_EINVAL, "fl_slab_begin not called");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  fl_slab* g0 = slabs[0];  // its side stream and events serve the group
+  cudaStream_t side = g0->side;
+  auto ok = [](cudaError_t e) {
+    return e == cudaSuccess ? FL_OK : fl::set_error(FL_ECUDA, "fl_slab_steps: %s",
+                                                    cudaGetErrorString(e));
+  };
+  // One sweep of every slab in three parts: the rows that need no ghost row
+  // (the interior, launched while the exchange runs on the side stream),
+  // then, once the exchange is in, the `reach` rows at each edge that faces
+  // a neighbour.
+  auto sweep = [&](int dim, int reach, cudaEvent_t exchanged) -> int {
+    int r = FL_OK;
+    for (int i = 0; i < count && r == FL_OK; ++i) {
+      fl_slab* s = slabs[i];
+      const int64_t lo = s->own_lo + (s->below ? reach : 0);
+      const int64_t hi = s->own_hi - (s->above ? reach : 0);
+      if (lo < hi)
+        r = fl::sim_sweep_part(s->sim, dim, lo, hi, s->counters + (dim * 3 + 0) * 2, s->parity,
+                               0, stream);
+    }
+    if (r == FL_OK) r = ok(cudaStreamWaitEvent(st, exchanged, 0));
+    for (int i = 0; i < count && r == FL_OK; ++i) {
+      fl_slab* s = slabs[i];
+      const int64_t lo = s->own_lo + (s->below ? reach : 0);
+      const int64_t hi = s->own_hi - (s->above ? reach : 0);
+      const int64_t bot_hi = lo < s->own_hi ? lo : s->own_hi;
+      const int64_t top_lo = hi > bot_hi ? hi : bot_hi;
+      r = fl::sim_sweep_part(s->sim, dim, s->own_lo, bot_hi, s->counters + (dim * 3 + 1) * 2,
+                             s->parity, 0, stream);
+      if (r == FL_OK)
+        r = fl::sim_sweep_part(s->sim, dim, top_lo, s->own_hi, s->counters + (dim * 3 + 2) * 2,
+                               s->parity, 1, stream);
+    }
+    return r;
+  };
   for (int64_t k = 0; k < nsteps; ++k) {
-    rc = exchange(slabs, count, 0, kRowsX, st);
-    for (int i = 0; i < count && rc == FL_OK; ++i) rc = fl_sim_sweep(slabs[i]->sim, 0, stream);
-    if (rc == FL_OK) rc = exchange(slabs, count, 1, kRowsY, st);
-    for (int i = 0; i < count && rc == FL_OK; ++i) rc = fl_sim_sweep(slabs[i]->sim, 1, stream);
-    if (rc == FL_OK) rc = reduce_words(slabs, count, st);
+    for (int i = 0; i < count && rc == FL_OK; ++i)
+      if (slabs[i]->counters_dirty) {
+        rc = ok(cudaMemsetAsync(slabs[i]->counters, 0, kParts * 2 * sizeof(unsigned int), st));
+        if (rc == FL_OK) slabs[i]->counters_dirty = false;
+      }
+    // x sweep: exchange 3 ghost rows of a on the side stream meanwhile
+    if (rc == FL_OK) rc = ok(cudaEventRecord(g0->ev[0], st));
+    if (rc == FL_OK) rc = ok(cudaStreamWaitEvent(side, g0->ev[0], 0));
+    if (rc == FL_OK) rc = exchange(slabs, count, 0, kRowsX, side);
+    if (rc == FL_OK) rc = ok(cudaEventRecord(g0->ev[1], side));
+    if (rc == FL_OK) rc = sweep(0, kRowsX, g0->ev[1]);
+    // y sweep: exchange 4 ghost rows of b (written by the x sweep's edges)
+    if (rc == FL_OK) rc = ok(cudaEventRecord(g0->ev[2], st));
+    if (rc == FL_OK) rc = ok(cudaStreamWaitEvent(side, g0->ev[2], 0));
+    if (rc == FL_OK) rc = exchange(slabs, count, 1, kRowsY, side);
+    if (rc == FL_OK) rc = ok(cudaEventRecord(g0->ev[3], side));
+    if (rc == FL_OK) rc = sweep(1, kRowsY, g0->ev[3]);
+    // the wavespeed maximum (NCCL on the side stream, after the y sweep),
+    // then the step
+    if (rc == FL_OK) {
+      if (g0->nccl) {
+        rc = ok(cudaEventRecord(g0->ev[0], st));
+        if (rc == FL_OK) rc = ok(cudaStreamWaitEvent(side, g0->ev[0], 0));
+        if (rc == FL_OK) rc = reduce_words(slabs, count, side);
+        if (rc == FL_OK) rc = ok(cudaEventRecord(g0->ev[1], side));
+        if (rc == FL_OK) rc = ok(cudaStreamWaitEvent(st, g0->ev[1], 0));
+      } else {
+        rc = reduce_words(slabs, count, st);
+      }
+    }
     for (int i = 0; i < count && rc == FL_OK; ++i) rc = fl_sim_finalize(slabs[i]->sim, 1, stream);
-    if (rc) return rc;
+    if (rc) {
+      for (int i = 0; i < count; ++i) slabs[i]->counters_dirty = true;
+      return rc;
+    }
+    for (int i = 0; i < count; ++i) slabs[i]->parity ^= 1;
   }
   return FL_OK;
 }
@@ -382,6 +463,10 @@ int fl_slab_steps(fl_slab* const* slabs, int count, int64_t nsteps, void* stream
 int fl_slab_destroy(fl_slab* slab) {
   if (slab == nullptr) return FL_OK;
   if (slab->comm != nullptr && nccl().ok) nccl().comm_destroy(slab->comm);
+  for (int i = 0; i < 4; ++i)
+    if (slab->ev[i] != nullptr) cudaEventDestroy(slab->ev[i]);
+  if (slab->side != nullptr) cudaStreamDestroy(slab->side);
+  if (slab->counters != nullptr) cudaFree(slab->counters);
   if (slab->word) cudaFree(slab->word);
   if (slab->sim) fl_sim_destroy(slab->sim);
   delete slab;

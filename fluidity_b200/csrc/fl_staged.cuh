@@ -462,7 +462,11 @@ __global__ void __launch_bounds__(StagedCfg<T, GEO, TOUT>::THREADS,
   const bool want_ws = (p.ws_accum != nullptr);
   const int ry = (p.walk_ry > 0) ? p.walk_ry : Cf::RY;
   const int64_t nab = (p.n[1 - S] + 31) / 32;
-  const int64_t items = nab * ((p.n[S] + ry - 1) / ry);
+  // positions along the walk to compute: a row window when the walk runs
+  // along the rows (the y sweep in the grid's own layout), else all
+  const bool win = S == 1 && !p.transposed && p.row_hi > p.row_lo;
+  const int64_t w_lo = win ? p.row_lo : 0, w_hi = win ? p.row_hi : p.n[S];
+  const int64_t items = nab * ((w_hi - w_lo + ry - 1) / ry);
   uint32_t gstage = 0;
   int fault = 0;
   unsigned int* next = (p.walk_next != nullptr) ? &p.walk_next[p.walk_slot] : nullptr;
@@ -473,8 +477,10 @@ __global__ void __launch_bounds__(StagedCfg<T, GEO, TOUT>::THREADS,
     item = (int64_t)__shfl_sync(0xffffffffu, v, 0);
   }
   while (item < items && !fault) {
+    const int64_t s0 = w_lo + (item / nab) * ry;
     staged_strip<T, S, FLUX, GEO, TOUT>(p, &tin, &tout, sm, dtdh, dhdt, (int)(item % nab),
-                             (int)((item / nab) * ry), ry, ws_local, want_ws, gstage, fault);
+                                        (int)s0, (int)(w_hi - s0 < ry ? w_hi - s0 : ry),
+                                        ws_local, want_ws, gstage, fault);
     if (next == nullptr) break;
     unsigned int v = 0u;
     if (lane == 0) v = atomicAdd(next, 1u);

@@ -283,21 +283,27 @@ walk_kernel_2d(SweepParams p) {
   const int warp = threadIdx.x >> 5;
   double ws_local = 0.0;
   const bool want_ws = (p.ws_accum != nullptr);
+  // the rows to compute: [r_lo, r_hi)
+  const bool win = p.row_hi > p.row_lo;
+  const int64_t r_lo = win ? p.row_lo : 0, r_hi = win ? p.row_hi : p.n[1];
   if (p.walk_next == nullptr) {
-    const int64_t y0 = ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
-    walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0, W::RY, ws_local, want_ws);
+    const int64_t y0 = r_lo + ((int64_t)blockIdx.y * W::WARPS + warp) * W::RY;
+    if (y0 < r_hi)
+      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)blockIdx.x, y0,
+                                (int)(r_hi - y0 < W::RY ? r_hi - y0 : W::RY), ws_local, want_ws);
   } else {
     const int ry = (p.walk_ry > 0) ? p.walk_ry : W::RY;
     const int64_t ncol = (p.n[0] + W::OWN - 1) / W::OWN;
-    const int64_t items = ncol * ((p.n[1] + ry - 1) / ry);
+    const int64_t items = ncol * ((r_hi - r_lo + ry - 1) / ry);
     unsigned int* next = &p.walk_next[p.walk_slot];
     for (;;) {
       unsigned int item = 0u;
       if ((threadIdx.x & 31) == 0) item = atomicAdd(next, 1u);
       item = __shfl_sync(0xffffffffu, item, 0);
       if ((int64_t)item >= items) break;
-      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)item % ncol, ((int64_t)item / ncol) * ry, ry,
-                                ws_local, want_ws);
+      const int64_t y0 = r_lo + ((int64_t)item / ncol) * ry;
+      walk_strip_2d<T, S, FLUX>(p, dtdh, (int64_t)item % ncol, y0,
+                                (int)(r_hi - y0 < ry ? r_hi - y0 : ry), ws_local, want_ws);
     }
   }
   if (want_ws) {

@@ -89,11 +89,14 @@ def _gather(layouts, bufs, like):
 
 
 @pytest.mark.parametrize("dtype,world,shape", [("f64", 2, (96, 72)), ("f32", 3, (64, 45)),
-                                               ("f64", 4, (40, 64))])
+                                               ("f64", 4, (40, 64)), ("f64", 8, (32, 40))])
 def test_native_slab_steps_match_undivided_run(cuda, dtype, world, shape):
     """fl_slab_steps with in-process slabs: the whole decomposed step (3-row
     exchange, x sweep, 4-row exchange, y sweep, wavespeed maximum, finalize)
-    enqueued by one call, bit for bit the undivided run."""
+    enqueued by one call, each sweep in parts (the rows that need no ghost
+    row while the exchange runs on the side stream, then the edge rows),
+    bit for bit the undivided run.  8 slabs of 40 rows have 5 own rows each,
+    fewer than the two edges' 3 + 3 or 4 + 4."""
     from fluidity_b200.slab import NativeSlabs, SlabLayout
     T = 8
     u0, want, rt = _undivided(dtype, shape, T)
