@@ -20,9 +20,10 @@
 //    relaxes to the fixed point of the Godunov local eikonal solve
 //    (schemes/godunov_upwind_scheme.hpp:44-53); 16x16 tiles relax in shared
 //    memory, passes ping-pong between two buffers, only tiles stamped by a
-//    changed neighbour relax in the next pass (a worklist; the others hold
-//    the same values in both buffers), and the host checks convergence once
-//    per 16 passes; the result takes the
+//    changed neighbour relax in the next pass (a worklist: a changed tile
+//    and those of its 4 edge neighbours whose shared edge changed; the
+//    others hold the same values in both buffers), and the host checks
+//    convergence once per 16 passes; the result takes the
 //    input's sign (set_signs, :96-112).
 // FP64 level sets on 2-D grids; out-of-domain reads mirror the domain.
 #include <cuda_runtime.h>
@@ -118,6 +119,7 @@ __global__ void fim_init_kernel(const double* phi, int64_t nx, int64_t ny, doubl
   }
 }
 
+// Godunov upwind local solve (godunov_upwind_scheme.hpp:44-53).
 __device__ __forceinline__ double eik_local(double xm, double xp, double ym, double yp, double h) {
   const double a = dmin_(xm, xp), b = dmin_(ym, yp);
   const double fh = 1.0 * h;
@@ -128,8 +130,8 @@ __device__ __forceinline__ double eik_local(double xm, double xp, double ym, dou
 
 // Pass k over a worklist of tiles: reads src (the previous pass) and writes
 // dst.  Pass 0 relaxes every tile; pass k > 0 relaxes the tiles that a tile
-// which changed in pass k - 1 stamped (itself and its eight neighbours),
-// each listed once.  A relaxing tile loads itself and a one-cell halo (+max
+// which changed in pass k - 1 stamped (itself, and each of its 4 edge
+// neighbours whose shared edge changed), each listed once.  A relaxing tile loads itself and a one-cell halo (+max
 // outside the domain), relaxes FIM_INNER rounds in shared memory and writes
 // its cells to dst.  A tile off the list holds the same values in both
 // buffers: it last relaxed without a change (a tile that changes always
@@ -186,17 +188,25 @@ __global__ void __launch_bounds__(FT * FT) fim_pass_kernel(
       if (!__syncthreads_or(upd)) break;
     }
     if (in) dst[ci] = s[ly + 1][lx + 1];
-    if (mine) changed = 1;
+    // bit 0: a cell of the tile changed (the tile relaxes again next pass,
+    // which also brings the other buffer up to date); bits 1-4: a changed
+    // cell on the left, right, lower, upper edge.  The local solve reads the
+    // 4 edge neighbours only, so only the edge-adjacent tiles whose shared
+    // edge changed need the next pass.
+    if (mine)
+      atomicOr(&changed, 1 | (lx == 0 ? 2 : 0) | (lx == FT - 1 ? 4 : 0) | (ly == 0 ? 8 : 0) |
+                             (ly == FT - 1 ? 16 : 0));
     __syncthreads();
     if (threadIdx.x == 0 && changed) {
       atomicMax(last_change, k);
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int ax = tx0 + dx, ay = ty0 + dy;
-          if (ax < 0 || ax >= tiles_x || ay < 0 || ay >= tiles_y) continue;
-          const int nt = ay * tiles_x + ax;
-          if (atomicMax(stamp + nt, k + 1) < k + 1) next[atomicAdd(next_count, 1)] = nt;
-        }
+      const int dxs[5] = {0, -1, 1, 0, 0}, dys[5] = {0, 0, 0, -1, 1};
+      for (int q = 0; q < 5; ++q) {
+        if (!(changed & (1 << q))) continue;
+        const int ax = tx0 + dxs[q], ay = ty0 + dys[q];
+        if (ax < 0 || ax >= tiles_x || ay < 0 || ay >= tiles_y) continue;
+        const int nt = ay * tiles_x + ax;
+        if (atomicMax(stamp + nt, k + 1) < k + 1) next[atomicAdd(next_count, 1)] = nt;
+      }
     }
     __syncthreads();   // s and changed are reused by the next tile
   }
