@@ -461,9 +461,13 @@ using namespace fl;
 
 struct fl_mm {
   fl_grid grid;
-  unsigned int* walk_next = nullptr;  // strip counters of the split sweeps (2, device)
-  int64_t walk_launches = 0;          // sweeps launched with them: the parity slot
-  bool counters_dirty = false;        // a counted sweep failed: re-zero both first
+  // strip counters of the split sweeps, a pair per material (4, device)
+  unsigned int* walk_next = nullptr;
+  int64_t walk_launches = 0;          // sweeps launched per material: the parity slot
+  bool counters_dirty = false;        // a counted sweep failed: re-zero them first
+  // material 1's split step runs on a stream of its own, beside material 0's
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   uint32_t policy;
   bool f32;
   double gamma[2];
@@ -499,6 +503,9 @@ void free_mm(fl_mm* m) {
   if (!m) return;
   cudaFree(m->cnt);
   cudaFree(m->walk_next);
+  if (m->fork) cudaEventDestroy(m->fork);
+  if (m->join) cudaEventDestroy(m->join);
+  if (m->side) cudaStreamDestroy(m->side);
   for (int k = 0; k < 2; ++k) {
     cudaFree(m->band_list[k]);
     cudaFree(m->gfm_idx[k]);
@@ -620,8 +627,11 @@ int fl_mm_create(fl_mm** out, const fl_grid* grid, const double* gammas, uint32_
   const int64_t n = grid->n[0] * grid->n[1];
   const int64_t lsb = fl_ls_workspace_bytes(grid);
   cudaError_t e = cudaMalloc(&m->cnt, sizeof(MMCounters));
-  if (e == cudaSuccess) e = cudaMalloc(&m->walk_next, 2 * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMemset(m->walk_next, 0, 2 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&m->walk_next, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(m->walk_next, 0, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->join, cudaEventDisableTiming);
   for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
     e = cudaMalloc(&m->band_list[k], n * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&m->gfm_idx[k], n * sizeof(int));
@@ -822,22 +832,38 @@ int fl_mm_steps(fl_mm* m, int64_t nsteps, void* stream) {
     const double dtdh = dt / m->h;
     // 4: each material's split step with its own gamma; state returns to buffer 0
     // split_solver.cuh:67-79 per material: sweep x into the second buffer,
-    // y back into the first, with strip counters of their own
-    for (int mat = 0; mat < 2; ++mat) {
-      const fl_material mm{m->gamma[mat], m->pinf[mat]};
-      for (int d = 0; d < 2 && rc == 0; ++d) {
-        void* in = m->u[mat][d];
-        void* out = m->u[mat][1 - d];
-        if (m->counters_dirty) {
-          const cudaError_t ce = cudaMemsetAsync(m->walk_next, 0, 2 * sizeof(unsigned int), st);
-          if (ce != cudaSuccess) return cuda_err(ce, "fl_mm_steps");
-          m->counters_dirty = false;
-        }
-        rc = split_sweep_counted(g, d, in, out, &mm, dtdh, m->policy, 0u, nullptr,
-                                 m->walk_next, (int)(m->walk_launches++ & 1), stream);
-        if (rc) m->counters_dirty = true;
+    // y back into the first, with strip counters of their own.  The two
+    // materials' steps are independent: material 1's runs on the side
+    // stream while material 0's runs on the loop's, which fills the GPU
+    // better than one 2.1M-cell sweep at a time.
+    if (m->counters_dirty) {
+      const cudaError_t ce = cudaMemsetAsync(m->walk_next, 0, 4 * sizeof(unsigned int), st);
+      if (ce != cudaSuccess) return cuda_err(ce, "fl_mm_steps");
+      m->counters_dirty = false;
+    }
+    {
+      cudaError_t ce = cudaEventRecord(m->fork, st);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(m->side, m->fork, 0);
+      if (ce != cudaSuccess) return cuda_err(ce, "fl_mm_steps");
+    }
+    for (int d = 0; d < 2 && rc == 0; ++d) {
+      const int slot = (int)(m->walk_launches & 1);
+      for (int mat = 0; mat < 2 && rc == 0; ++mat) {
+        const fl_material mm{m->gamma[mat], m->pinf[mat]};
+        rc = split_sweep_counted(g, d, m->u[mat][d], m->u[mat][1 - d], &mm, dtdh, m->policy, 0u,
+                                 nullptr, m->walk_next + 2 * mat, slot,
+                                 mat == 0 ? stream : static_cast<void*>(m->side));
       }
-      if (rc) return rc;
+      m->walk_launches += 1;
+    }
+    {
+      cudaError_t ce = cudaEventRecord(m->join, m->side);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, m->join, 0);
+      if (ce != cudaSuccess && rc == 0) rc = cuda_err(ce, "fl_mm_steps");
+    }
+    if (rc) {
+      m->counters_dirty = true;
+      return rc;
     }
     // 5: level sets (multimaterial_simulator.hpp:428-477)
     const double* phis[2] = {m->phi[0][m->phi_cur[0]], m->phi[1][m->phi_cur[1]]};
