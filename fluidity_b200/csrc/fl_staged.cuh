@@ -218,7 +218,10 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       stage_issue<T, GEO, TOUT>(sm, tin, (int)((g0 + t) % NS), k_first + t * PPS, nl, a0);
   }
 
-  // the stage holding walk offset r, and r's column within it
+  // the stage holding walk offset r, and r's column within it.  With one
+  // position per stage the walk's own stage slot advances by one per row
+  // (slot_r below), and the rows behind it are slots back from it.
+  int slot_r = (int)(g0 % NS);   // ring slot of the stage of walk offset r
   auto stage_of = [&](int r, int& q) -> const T* {
     const int t = r / PPS;
     q = r - t * PPS;
@@ -228,6 +231,15 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       if (rev) q = PPS - 1 - q;
     }
     return sm.ring + (size_t)((g0 + t) % NS) * Cf::STAGE;
+  };
+  auto stage_back = [&](int r, int back, int& q) -> const T* {
+    if (GEO) {
+      q = 0;
+      int sl = slot_r - back;
+      if (sl < 0) sl += NS;
+      return sm.ring + (size_t)sl * Cf::STAGE;
+    }
+    return stage_of(r - back, q);
   };
   // the cell at box index a of a stage, with the ghost flips: gl along the
   // sweep (a mirrored position), fx across it (a mirrored lane)
@@ -281,8 +293,9 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       }
     }
     // ---- derive position k: own cell, then the across halo ---------------
+    if (GEO && r > 0) slot_r = (slot_r + 1 == NS) ? 0 : slot_r + 1;
     int qk;
-    const T* stk = stage_of(r, qk);
+    const T* stk = stage_back(r, 0, qk);
     const bool glk = ghost_l(k);
     const Cons<T, D> u = load(stk, qk, aoff, glk, flip_a);
     const Derived<T, D> q = derive(u, gm1);
@@ -330,8 +343,8 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     if (j < s0 - 1) continue;
     // ---- evolved face states of (lane, j) ----------------------------------
     int qj, qm;
-    const T* stj = stage_of(r - 3, qj);
-    const T* stm = stage_of(r - 4, qm);
+    const T* stj = stage_back(r, 3, qj);
+    const T* stm = stage_back(r, 4, qm);
     const Cons<T, D> uj = load(stj, qj, aoff, ghost_l(j), flip_a);
     const Cons<T, D> um = load(stm, qm, aoff, ghost_l(j - 1), flip_a);  // position j - 1
     Cons<T, D> er, el;
@@ -340,7 +353,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       el = uj;
     } else {
       int qp;
-      const T* stp = stage_of(r - 2, qp);
+      const T* stp = stage_back(r, 2, qp);
       const Cons<T, D> up = load(stp, qp, aoff, ghost_l(j + 1), flip_a);
       T chi_v = T(1);
       if (flatten) {
@@ -351,11 +364,21 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       }
       const T ch = chi_v * T(0.5);
       Cons<T, D> a, b;
+      // one test of the limiter kind per position, not per component
+      if (p.limiter == kSuperbee) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const T delta = ch * limited_slope<T>(p.limiter, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
-        a.v[c] = uj.v[c] - delta;
-        b.v[c] = uj.v[c] + delta;
+        for (int c = 0; c < NC; ++c) {
+          const T delta = ch * limited_slope<T>(kSuperbee, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
+          a.v[c] = uj.v[c] - delta;
+          b.v[c] = uj.v[c] + delta;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const T delta = ch * limited_slope<T>(kVanLeer, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
+          a.v[c] = uj.v[c] - delta;
+          b.v[c] = uj.v[c] + delta;
+        }
       }
       Cons<T, D> fa, fb;
       flux_q(a, derive(a, gm1), S, fa);
