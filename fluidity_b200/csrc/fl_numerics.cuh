@@ -228,10 +228,11 @@ FL_HD T limit_single(int limiter, T left, T right) {
   return (r <= T(0) || right == T(0)) ? T(0) : T(2) * std_min(r, T(1)) / (T(1) + r);
 }
 
-// FL_FAST_DIV 1 (the default): the HLLC star speed, star scale and energy
-// term multiply by one reciprocal instead of dividing, and the flattening
-// threshold test compares a product; results differ from the divisions by
-// rounding (measured 2.6% faster in the FP64 sweep).
+// FL_FAST_DIV 1 (the default): the HLLC star speed, star scale, energy
+// term and shock pressure ratios multiply by one reciprocal instead of
+// dividing, and the flattening threshold test compares a product; results
+// differ from the divisions by rounding (measured 2.6% faster in the FP64
+// sweep before the shock ratios joined).
 #ifndef FL_FAST_DIV
 #define FL_FAST_DIV 1
 #endif
@@ -390,11 +391,22 @@ FL_HD void hllc_q(const Cons<T, D>& ul, const Derived<T, D>& ql,
   const T ar = fl_ksqrt<T>(gamma * sound_p<STIFF>(pr, pinf) * qr.rinv);
   const T p_pvrs = T(0.5) * ((pl + pr) - (T(0.25) * (vr - vl) * (ur.v[0] + ul.v[0]) * (al + ar)));
   const T p_star = std_max(T(0), p_pvrs);
+#if FL_FAST_DIV
+  // the shock speeds' pressure ratios by reciprocal (rounding-level change)
+  const T wsl = (p_star <= pl)
+                    ? vl + (-al)
+                    : vl + (-al) * fl_ksqrt<T>(T(1) + adi * (p_star * fl_rcp<T>(pl) - T(1)));
+  if (T(0) <= wsl) { flux_vp(ul, d, vl, pl, f); return; }
+  const T wsr = (p_star <= pr)
+                    ? vr + ar
+                    : vr + ar * fl_ksqrt<T>(T(1) + adi * (p_star * fl_rcp<T>(pr) - T(1)));
+#else
   const T wsl = (p_star <= pl) ? vl + (-al)
                                : vl + (-al) * fl_ksqrt<T>(T(1) + adi * (p_star / pl - T(1)));
   if (T(0) <= wsl) { flux_vp(ul, d, vl, pl, f); return; }
   const T wsr = (p_star <= pr) ? vr + ar
                                : vr + ar * fl_ksqrt<T>(T(1) + adi * (p_star / pr - T(1)));
+#endif
   if (T(0) >= wsr) { flux_vp(ur, d, vr, pr, f); return; }
   const T factl = ul.v[0] * (wsl - vl);
   const T factr = ur.v[0] * (wsr - vr);
