@@ -23,6 +23,7 @@
 #pragma once
 
 #include <cfloat>
+#include <type_traits>
 
 #include "fl_internal.cuh"
 #include "fl_numerics.cuh"
@@ -180,20 +181,28 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
         }
         const T ch = chi_v * T(0.5);
         Cons<T, D> a, b;
+        // the limiter kind tested once per position, not per component
+        auto slopes = [&](auto lim) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          T um, up;
-          if (S == 0) {
-            um = shfl_up(u.v[c], 1);
-            up = shfl_dn(u.v[c], 1);
-          } else {
-            um = U[0].v[c];
-            up = U[2].v[c];
+          for (int c = 0; c < NC; ++c) {
+            T um, up;
+            if (S == 0) {
+              um = shfl_up(u.v[c], 1);
+              up = shfl_dn(u.v[c], 1);
+            } else {
+              um = U[0].v[c];
+              up = U[2].v[c];
+            }
+            const T delta =
+                ch * limited_slope<T>(decltype(lim)::value, u.v[c] - um, up - u.v[c]);
+            a.v[c] = u.v[c] - delta;
+            b.v[c] = u.v[c] + delta;
           }
-          const T delta = ch * limited_slope<T>(p.limiter, u.v[c] - um, up - u.v[c]);
-          a.v[c] = u.v[c] - delta;
-          b.v[c] = u.v[c] + delta;
-        }
+        };
+        if (p.limiter == kSuperbee)
+          slopes(std::integral_constant<int, kSuperbee>{});
+        else
+          slopes(std::integral_constant<int, kVanLeer>{});
         Cons<T, D> fa, fb;
         flux_q(a, derive(a, gm1), S, fa);
         flux_q(b, derive(b, gm1), S, fb);
