@@ -17,6 +17,8 @@
 //   control.
 #pragma once
 
+#include <type_traits>
+
 #include <cfloat>
 
 #include "fl_internal.cuh"
@@ -199,12 +201,20 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
       }
       const T ch = chi_v * T(0.5);
       Cons<T, D> aa, bb;
+      // the limiter kind tested once per position, not per component
+      auto slopes = [&](auto lim) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const T delta = ch * limited_slope<T>(limiter, uj.v[c] - U[0].v[c], U[2].v[c] - uj.v[c]);
-        aa.v[c] = uj.v[c] - delta;
-        bb.v[c] = uj.v[c] + delta;
-      }
+        for (int c = 0; c < NC; ++c) {
+          const T delta = ch * limited_slope<T>(decltype(lim)::value, uj.v[c] - U[0].v[c],
+                                                U[2].v[c] - uj.v[c]);
+          aa.v[c] = uj.v[c] - delta;
+          bb.v[c] = uj.v[c] + delta;
+        }
+      };
+      if (limiter == kSuperbee)
+        slopes(std::integral_constant<int, kSuperbee>{});
+      else
+        slopes(std::integral_constant<int, kVanLeer>{});
       Cons<T, D> fa, fb;
       flux_q(aa, derive(aa, gm1), 0, fa);
       flux_q(bb, derive(bb, gm1), 0, fb);
