@@ -168,6 +168,8 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
   T P[5], V[5];
   T CH[3];
   Cons<T, D> er_prev, f_prev;
+  // the walk, with the limiter kind fixed for the whole row
+  auto walk = [&](auto lim) {
   for (int k = c0 - 4; k <= c1 + 3; ++k) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -201,8 +203,6 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
       }
       const T ch = chi_v * T(0.5);
       Cons<T, D> aa, bb;
-      // the limiter kind tested once per position, not per component
-      auto slopes = [&](auto lim) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const T delta = ch * limited_slope<T>(decltype(lim)::value, uj.v[c] - U[0].v[c],
@@ -210,11 +210,6 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
           aa.v[c] = uj.v[c] - delta;
           bb.v[c] = uj.v[c] + delta;
         }
-      };
-      if (limiter == kSuperbee)
-        slopes(std::integral_constant<int, kSuperbee>{});
-      else
-        slopes(std::integral_constant<int, kVanLeer>{});
       Cons<T, D> fa, fb;
       flux_q(aa, derive(aa, gm1), 0, fa);
       flux_q(bb, derive(bb, gm1), 0, fb);
@@ -242,6 +237,11 @@ __device__ __forceinline__ void walk_line_1d(const T* src, T* dst, int ld, int c
     }
     er_prev = er;
   }
+  };
+  if (limiter == kSuperbee)
+    walk(std::integral_constant<int, kSuperbee>{});
+  else
+    walk(std::integral_constant<int, kVanLeer>{});
 }
 
 template <typename T>

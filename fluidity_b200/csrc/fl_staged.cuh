@@ -21,7 +21,8 @@
 // sweep reads the ring (own lane only, no exchange).  The stencil across the
 // sweep -- the flattening coefficient's pressure and velocity reach of 3 --
 // goes through three small per-warp exchange rows; the 6 across-halo cells
-// (3 on each side of the warp) are derived by lanes 0-5 in one extra pass.
+// (3 on each side of the warp) are derived in one extra pass of all lanes, of
+// which lanes 0-5 keep theirs (no divergent region).
 // The reference's halo of 4 along the sweep costs 7 extra derivations per
 // strip of 64 and one extra evolve and Riemann solve at its start.
 //
@@ -33,6 +34,7 @@
 #pragma once
 
 #include <cfloat>
+#include <type_traits>
 
 #include "fl_internal.cuh"
 #include "fl_numerics.cuh"
@@ -269,6 +271,9 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   T* const out = static_cast<T*>(p.out);
   const int64_t pitch = p.pitch;
 
+  // the walk, with the limiter kind fixed for the whole strip
+  auto walk = [&](auto lim) {
+  constexpr int LIM = decltype(lim)::value;
   for (int r = 0; r < nr; ++r) {
     const int k = k_first + r;
     // ---- ring: recycle the stage the walk no longer reads, wait for k ----
@@ -310,21 +315,27 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     if (flatten) {
       sm.xp[own] = q.p;
       sm.xv[own] = q.v[1 - S];
-      if (lane < 6) {
+      {
+        // every lane derives a halo cell (lanes 0-5 keep theirs): no
+        // divergent region between the own and the halo derivations
         const Cons<T, D> uh = load(stk, qk, hoff, glk, flip_h);
         const Derived<T, D> qh = derive(uh, gm1);
-        sm.xp[hx] = qh.p;
-        sm.xv[hx] = qh.v[1 - S];
+        if (lane < 6) {
+          sm.xp[hx] = qh.p;
+          sm.xv[hx] = qh.v[1 - S];
+        }
       }
       __syncwarp();
       const T pr1 = sm.xp[own + 1], pl1 = sm.xp[own - 1];
       const T chx = (T)chi_base<T>(pr1, pl1, sm.xp[own + 2], sm.xp[own - 2], sm.xv[own - 1],
                                    sm.xv[own + 1]);
       sm.xc[own] = chx;
-      if (lane < 2) {
+      {
+        // lanes 0 and 1: the flattening base just outside the warp
         const int o = (lane == 0) ? Cf::AOFF - 1 : Cf::AOFF + 32;
-        sm.xc[o] = (T)chi_base<T>(sm.xp[o + 1], sm.xp[o - 1], sm.xp[o + 2], sm.xp[o - 2],
-                                  sm.xv[o - 1], sm.xv[o + 1]);
+        const T ce = (T)chi_base<T>(sm.xp[o + 1], sm.xp[o - 1], sm.xp[o + 2], sm.xp[o - 2],
+                                    sm.xv[o - 1], sm.xv[o + 1]);
+        if (lane < 2) sm.xc[o] = ce;
       }
       const T dx = pr1 - pl1;
       const int sx = (T(0) < dx) - (dx < T(0));
@@ -364,21 +375,11 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       }
       const T ch = chi_v * T(0.5);
       Cons<T, D> a, b;
-      // one test of the limiter kind per position, not per component
-      if (p.limiter == kSuperbee) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const T delta = ch * limited_slope<T>(kSuperbee, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
-          a.v[c] = uj.v[c] - delta;
-          b.v[c] = uj.v[c] + delta;
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const T delta = ch * limited_slope<T>(kVanLeer, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
-          a.v[c] = uj.v[c] - delta;
-          b.v[c] = uj.v[c] + delta;
-        }
+      for (int c = 0; c < NC; ++c) {
+        const T delta = ch * limited_slope<T>(LIM, uj.v[c] - um.v[c], up.v[c] - uj.v[c]);
+        a.v[c] = uj.v[c] - delta;
+        b.v[c] = uj.v[c] + delta;
       }
       Cons<T, D> fa, fb;
       flux_q(a, derive(a, gm1), S, fa);
@@ -441,6 +442,11 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     }
     er_prev = er;
   }
+  };
+  if (p.limiter == kSuperbee)
+    walk(std::integral_constant<int, kSuperbee>{});
+  else
+    walk(std::integral_constant<int, kVanLeer>{});
   if (fault) {
     // stop issuing; let every copy already issued land before the shared
     // memory is released (each wait bounded again)
