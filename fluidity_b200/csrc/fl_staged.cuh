@@ -271,9 +271,12 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   T* const out = static_cast<T*>(p.out);
   const int64_t pitch = p.pitch;
 
-  // the walk, with the limiter kind fixed for the whole strip
-  auto walk = [&](auto lim) {
+  // the walk, with the limiter kind fixed for the whole strip, and the
+  // reflective flips compiled out when neither end of either dimension
+  // reflects
+  auto walk = [&](auto lim, auto refl) {
   constexpr int LIM = decltype(lim)::value;
+  constexpr bool RF = decltype(refl)::value;
   for (int r = 0; r < nr; ++r) {
     const int k = k_first + r;
     // ---- ring: recycle the stage the walk no longer reads, wait for k ----
@@ -301,8 +304,8 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     if (GEO && r > 0) slot_r = (slot_r + 1 == NS) ? 0 : slot_r + 1;
     int qk;
     const T* stk = stage_back(r, 0, qk);
-    const bool glk = ghost_l(k);
-    const Cons<T, D> u = load(stk, qk, aoff, glk, flip_a);
+    const bool glk = RF && ghost_l(k);
+    const Cons<T, D> u = load(stk, qk, aoff, glk, RF && flip_a);
     const Derived<T, D> q = derive(u, gm1);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -318,7 +321,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       {
         // every lane derives a halo cell (lanes 0-5 keep theirs): no
         // divergent region between the own and the halo derivations
-        const Cons<T, D> uh = load(stk, qk, hoff, glk, flip_h);
+        const Cons<T, D> uh = load(stk, qk, hoff, glk, RF && flip_h);
         const Derived<T, D> qh = derive(uh, gm1);
         if (lane < 6) {
           sm.xp[hx] = qh.p;
@@ -356,8 +359,8 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     int qj, qm;
     const T* stj = stage_back(r, 3, qj);
     const T* stm = stage_back(r, 4, qm);
-    const Cons<T, D> uj = load(stj, qj, aoff, ghost_l(j), flip_a);
-    const Cons<T, D> um = load(stm, qm, aoff, ghost_l(j - 1), flip_a);  // position j - 1
+    const Cons<T, D> uj = load(stj, qj, aoff, RF && ghost_l(j), RF && flip_a);
+    const Cons<T, D> um = load(stm, qm, aoff, RF && ghost_l(j - 1), RF && flip_a);  // position j - 1
     Cons<T, D> er, el;
     if (!muscl) {
       er = uj;
@@ -365,7 +368,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     } else {
       int qp;
       const T* stp = stage_back(r, 2, qp);
-      const Cons<T, D> up = load(stp, qp, aoff, ghost_l(j + 1), flip_a);
+      const Cons<T, D> up = load(stp, qp, aoff, RF && ghost_l(j + 1), RF && flip_a);
       T chi_v = T(1);
       if (flatten) {
         const T dl = P[2] - P[0];
@@ -443,10 +446,19 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     er_prev = er;
   }
   };
-  if (p.limiter == kSuperbee)
-    walk(std::integral_constant<int, kSuperbee>{});
-  else
-    walk(std::integral_constant<int, kVanLeer>{});
+  using SB = std::integral_constant<int, kSuperbee>;
+  using VL_ = std::integral_constant<int, kVanLeer>;
+  if (flip_l_on || flip_a_on) {
+    if (p.limiter == kSuperbee)
+      walk(SB{}, std::true_type{});
+    else
+      walk(VL_{}, std::true_type{});
+  } else {
+    if (p.limiter == kSuperbee)
+      walk(SB{}, std::false_type{});
+    else
+      walk(VL_{}, std::false_type{});
+  }
   if (fault) {
     // stop issuing; let every copy already issued land before the shared
     // memory is released (each wait bounded again)
