@@ -94,13 +94,13 @@ def workload_config(a):
 
 
 def alternating_transposes(a):
-    """Plane transposes per run of the device-resident loop: the FP64 HLLC
-    2-D loop alternates layouts (state in, then back out) when both extents
-    are multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set;
-    "staged" extends it to every dtype and flux."""
+    """Plane transposes per run of the device-resident loop: the FP64 2-D
+    loop alternates layouts (state in, then back out) when both extents are
+    multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set;
+    "staged" extends it to FP32."""
     mode = os.environ.get("FLUIDITY_B200_SWEEP", "")
     elem = 8 if a.dtype == "f64" else 4
-    on = (mode == "staged") or (mode == "" and a.dtype == "f64" and a.flux == "hllc")
+    on = (mode == "staged") or (mode == "" and a.dtype == "f64")
     return 2 if on and (a.size * elem) % 16 == 0 else 0
 
 

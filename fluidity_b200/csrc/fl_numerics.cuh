@@ -236,37 +236,14 @@ FL_HD T limit_single(int limiter, T left, T right) {
 #ifndef FL_FAST_DIV
 #define FL_FAST_DIV 1
 #endif
-
-// ---- flattening (reconstruction/muscl_reconstructor.hpp:59-87) ----------
-// Inputs: pressures at c+1, c-1, c+2, c-2 and velocities (sweep of chi's own
-// dimension) at c-1, c+1.  Ratio in T; sigma test and eta in double.
-
-template <typename T>
-FL_HD double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
-                                           T u_prev, T u_next) {
-  const T u_factor = u_prev - u_next;
-  const T dp = fl_abs<T>(p_next - p_prev);
-#if FL_FAST_DIV
-  // the ratio test as a product: differs from the division only where
-  // dp / min(p) is within an ulp of 0.33
-#if FL_FAST_F32
-  const bool flatten = sizeof(T) == 4
-                           ? (u_factor > T(0) && dp > T(0.33) * std_min(p_next, p_prev))
-                           : ((double)u_factor > 0.0 &&
-                              (double)dp > 0.33 * (double)std_min(p_next, p_prev));
-#else
-  const bool flatten = ((double)u_factor > 0.0) &&
-                       ((double)dp > 0.33 * (double)std_min(p_next, p_prev));
+// FL_CHI_FAST 1 (the default): in FP64 the flattening ratio z and its ramp
+// multiply by reciprocals (the ramp's a compile-time constant) instead of
+// dividing: a rounding-level change that takes the divisions' inlined code
+// out of every sweep's loop body (+1.6% on the FP64 sweep).  FP32 keeps its
+// divisions.
+#ifndef FL_CHI_FAST
+#define FL_CHI_FAST 1
 #endif
-#else
-  const bool flatten = ((double)u_factor > 0.0) && ((double)(dp / std_min(p_next, p_prev)) > 0.33);
-#endif
-  if (!flatten) return 1.0;
-  const T z = dp / fl_abs<T>(p_nnext - p_pprev);
-  const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
-  return std_min(1.0, std_max(0.0, temp));
-}
-
 
 // ---- fast forms used by the sweep kernel ---------------------------------
 // One reciprocal per state replaces the reference's one division per
@@ -343,6 +320,45 @@ template <> FL_HD float fl_ksqrt<float>(float x) {
   return r;
 }
 #endif
+
+// ---- flattening (reconstruction/muscl_reconstructor.hpp:59-87) ----------
+// Inputs: pressures at c+1, c-1, c+2, c-2 and velocities (sweep of chi's own
+// dimension) at c-1, c+1.  Ratio in T; sigma test and eta in double.
+
+template <typename T>
+FL_HD double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
+                                           T u_prev, T u_next) {
+  const T u_factor = u_prev - u_next;
+  const T dp = fl_abs<T>(p_next - p_prev);
+#if FL_FAST_DIV
+  // the ratio test as a product: differs from the division only where
+  // dp / min(p) is within an ulp of 0.33
+#if FL_FAST_F32
+  const bool flatten = sizeof(T) == 4
+                           ? (u_factor > T(0) && dp > T(0.33) * std_min(p_next, p_prev))
+                           : ((double)u_factor > 0.0 &&
+                              (double)dp > 0.33 * (double)std_min(p_next, p_prev));
+#else
+  const bool flatten = ((double)u_factor > 0.0) &&
+                       ((double)dp > 0.33 * (double)std_min(p_next, p_prev));
+#endif
+#else
+  const bool flatten = ((double)u_factor > 0.0) && ((double)(dp / std_min(p_next, p_prev)) > 0.33);
+#endif
+  if (!flatten) return 1.0;
+#if FL_CHI_FAST
+  if constexpr (sizeof(T) == 8) {
+    constexpr double kInvRamp = 1.0 / (0.85 - 0.75);
+    const T z = dp * fl_rcp<T>(fl_abs<T>(p_nnext - p_pprev));
+    const double temp = 1.0 - (((double)z - 0.75) * kInvRamp);
+    return std_min(1.0, std_max(0.0, temp));
+  }
+#endif
+  const T z = dp / fl_abs<T>(p_nnext - p_pprev);
+  const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
+  return std_min(1.0, std_max(0.0, temp));
+}
+
 
 // Primitive quantities derived from a conservative state.
 template <typename T, int D>

@@ -116,6 +116,9 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     bool f = false;
     ct_pre = __ldg(xc + base + mirror_index(k_first - 3, nr, f) * rs + gx);
   }
+  // the walk, with the reflective flips compiled out when no end reflects
+  auto walk = [&](auto refl) {
+  constexpr bool RF = decltype(refl)::value;
   for (int64_t k = k_first; k <= k_last; ++k) {
     const T ct = ct_pre;
     if (flatten && k < k_last) {
@@ -139,8 +142,8 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
 #pragma unroll
         for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + base + gy * rs + gx);
       }
-      if (flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
-      if (fy && flip_r_on) u.v[2 + DR] = (-(u.v[2 + DR] / u.v[0])) * u.v[0];
+      if (RF && flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
+      if (RF && fy && flip_r_on) u.v[2 + DR] = (-(u.v[2 + DR] / u.v[0])) * u.v[0];
       const Derived<T, D> q = derive(u, gm1);
       U[4] = u;
       P[4] = q.p;
@@ -265,6 +268,11 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
       er_prev = er;
     }
   }
+  };
+  if ((p.reflect & (1u | (1u << DR))) != 0)
+    walk(std::true_type{});
+  else
+    walk(std::false_type{});
 }
 
 template <typename T, int S, int FLUX>
