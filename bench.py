@@ -94,13 +94,13 @@ def workload_config(a):
 
 
 def alternating_transposes(a):
-    """Plane transposes per run of the device-resident loop: the FP64 2-D
-    loop alternates layouts (state in, then back out) when both extents are
-    multiples of 16 bytes and no FLUIDITY_B200_SWEEP override is set;
-    "staged" extends it to FP32."""
+    """Plane transposes per run of the device-resident loop: the 2-D loop in
+    FP64, and in FP32 with HLLC, alternates layouts (state in, then back out)
+    when both extents are multiples of 16 bytes and no FLUIDITY_B200_SWEEP
+    override is set; "staged" extends it to every dtype and flux."""
     mode = os.environ.get("FLUIDITY_B200_SWEEP", "")
     elem = 8 if a.dtype == "f64" else 4
-    on = (mode == "staged") or (mode == "" and a.dtype == "f64")
+    on = (mode == "staged") or (mode == "" and (a.dtype == "f64" or a.flux == "hllc"))
     return 2 if on and (a.size * elem) % 16 == 0 else 0
 
 

@@ -236,11 +236,11 @@ FL_HD T limit_single(int limiter, T left, T right) {
 #ifndef FL_FAST_DIV
 #define FL_FAST_DIV 1
 #endif
-// FL_CHI_FAST 1 (the default): in FP64 the flattening ratio z and its ramp
-// multiply by reciprocals (the ramp's a compile-time constant) instead of
-// dividing: a rounding-level change that takes the divisions' inlined code
-// out of every sweep's loop body (+1.6% on the FP64 sweep).  FP32 keeps its
-// divisions.
+// FL_CHI_FAST 1 (the default): the flattening ratio z and its ramp multiply
+// by reciprocals (the ramp's a compile-time constant) instead of dividing: a
+// rounding-level change that takes the divisions' inlined code out of every
+// sweep's loop body (+1.6% on the FP64 staged sweep, +3.3% on the FP32 one,
+// +4.6% on the batched kernel).
 #ifndef FL_CHI_FAST
 #define FL_CHI_FAST 1
 #endif
@@ -347,15 +347,13 @@ FL_HD double chi_base(T p_next, T p_prev, T p_nnext, T p_pprev,
 #endif
   if (!flatten) return 1.0;
 #if FL_CHI_FAST
-  if constexpr (sizeof(T) == 8) {
-    constexpr double kInvRamp = 1.0 / (0.85 - 0.75);
-    const T z = dp * fl_rcp<T>(fl_abs<T>(p_nnext - p_pprev));
-    const double temp = 1.0 - (((double)z - 0.75) * kInvRamp);
-    return std_min(1.0, std_max(0.0, temp));
-  }
-#endif
+  constexpr double kInvRamp = 1.0 / (0.85 - 0.75);
+  const T z = dp * fl_rcp<T>(fl_abs<T>(p_nnext - p_pprev));
+  const double temp = 1.0 - (((double)z - 0.75) * kInvRamp);
+#else
   const T z = dp / fl_abs<T>(p_nnext - p_pprev);
   const double temp = 1.0 - (((double)z - 0.75) / (0.85 - 0.75));
+#endif
   return std_min(1.0, std_max(0.0, temp));
 }
 
