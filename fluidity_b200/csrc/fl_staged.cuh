@@ -271,12 +271,15 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   T* const out = static_cast<T*>(p.out);
   const int64_t pitch = p.pitch;
 
-  // the walk, with the limiter kind fixed for the whole strip, and the
-  // reflective flips compiled out when neither end of either dimension
-  // reflects
-  auto walk = [&](auto lim, auto refl) {
+  // the walk, with the limiter kind fixed for the whole strip.  Its common
+  // form (FAST: no end of either dimension reflects, MUSCL with flattening)
+  // has the reflective flips and the reconstruction tests compiled out.
+  auto walk = [&](auto lim, auto fast) {
   constexpr int LIM = decltype(lim)::value;
-  constexpr bool RF = decltype(refl)::value;
+  constexpr bool FAST = decltype(fast)::value;
+  constexpr bool RF = !FAST;
+  const bool flat = FAST || flatten;
+  const bool mus = FAST || muscl;
   for (int r = 0; r < nr; ++r) {
     const int k = k_first + r;
     // ---- ring: recycle the stage the walk no longer reads, wait for k ----
@@ -315,7 +318,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     P[4] = q.p;
     VL[4] = q.v[S];
     T cx = T(1);
-    if (flatten) {
+    if (flat) {
       sm.xp[own] = q.p;
       sm.xv[own] = q.v[1 - S];
       {
@@ -351,7 +354,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     // ---- flattening base along the sweep of position k - 2 ---------------
     CHA[0] = CHA[1];
     CHA[1] = CHA[2];
-    if (flatten) CHA[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VL[1], VL[3]);
+    if (flat) CHA[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VL[1], VL[3]);
 
     const int j = k - 3;  // evolve position
     if (j < s0 - 1) continue;
@@ -362,7 +365,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
     const Cons<T, D> uj = load(stj, qj, aoff, RF && ghost_l(j), RF && flip_a);
     const Cons<T, D> um = load(stm, qm, aoff, RF && ghost_l(j - 1), RF && flip_a);  // position j - 1
     Cons<T, D> er, el;
-    if (!muscl) {
+    if (!mus) {
       er = uj;
       el = uj;
     } else {
@@ -370,7 +373,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       const T* stp = stage_back(r, 2, qp);
       const Cons<T, D> up = load(stp, qp, aoff, RF && ghost_l(j + 1), RF && flip_a);
       T chi_v = T(1);
-      if (flatten) {
+      if (flat) {
         const T dl = P[2] - P[0];
         const int sl = (T(0) < dl) - (dl < T(0));
         const T cl = std_min(CHA[1], sl > 0 ? CHA[2] : (sl < 0 ? CHA[0] : CHA[1]));
@@ -448,7 +451,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   };
   using SB = std::integral_constant<int, kSuperbee>;
   using VL_ = std::integral_constant<int, kVanLeer>;
-  if (flip_l_on || flip_a_on) {
+  if (!flip_l_on && !flip_a_on && flatten) {
     if (p.limiter == kSuperbee)
       walk(SB{}, std::true_type{});
     else
