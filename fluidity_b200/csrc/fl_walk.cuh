@@ -121,6 +121,13 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
 #pragma unroll
       for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
     }
+    // the walk; its common form (FAST: no reflective end in x or y, MUSCL
+    // with flattening) has the reflective flips and the reconstruction tests
+    // compiled out
+    auto walk = [&](auto fast) {
+    constexpr bool FAST = decltype(fast)::value;
+    const bool flat = FAST || flatten;
+    const bool mus = FAST || muscl;
     for (int64_t k = k_first; k <= k_last; ++k) {
       // ---- shift windows and take row k ----------------------------------
 #pragma unroll
@@ -138,8 +145,8 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
 #pragma unroll
           for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
         }
-        if (flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
-        if (fy && flip_y_on) u.v[3] = (-(u.v[3] / u.v[0])) * u.v[0];
+        if (!FAST && flip_x) u.v[2] = (-(u.v[2] / u.v[0])) * u.v[0];
+        if (!FAST && fy && flip_y_on) u.v[3] = (-(u.v[3] / u.v[0])) * u.v[0];
         const Derived<T, D> q = derive(u, gm1);
         U[4] = u;
         P[4] = q.p;
@@ -149,7 +156,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       // ---- y flattening base of row k - 2 (needs rows k-4..k) -----------
       CHY[0] = CHY[1];
       CHY[1] = CHY[2];
-      if (flatten) CHY[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VY[1], VY[3]);
+      if (flat) CHY[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], VY[1], VY[3]);
       const int64_t j = k - 3;  // evolve row
       const bool evolve_row = (S == 0) ? (j >= y0) : (j >= y0 - 1);
       if (!evolve_row) continue;
@@ -159,18 +166,18 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       const T p_r1 = shfl_dn(pj, 1), p_l1 = shfl_up(pj, 1);
       const T p_r2 = shfl_dn(pj, 2), p_l2 = shfl_up(pj, 2);
       T chx = T(1);
-      if (flatten) chx = (T)chi_base<T>(p_r1, p_l1, p_r2, p_l2, shfl_up(vxj, 1), shfl_dn(vxj, 1));
+      if (flat) chx = (T)chi_base<T>(p_r1, p_l1, p_r2, p_l2, shfl_up(vxj, 1), shfl_dn(vxj, 1));
       const T chx_r = shfl_dn(chx, 1), chx_l = shfl_up(chx, 1);
 
       // ---- evolved face states of (lane, j) -------------------------------
       const Cons<T, D>& u = U[1];
       Cons<T, D> er, el;
-      if (!muscl) {
+      if (!mus) {
         er = u;
         el = u;
       } else {
         T chi_v = T(1);
-        if (flatten) {
+        if (flat) {
           const T dx = p_r1 - p_l1;
           const int sx = (T(0) < dx) - (dx < T(0));
           const T cx = std_min(chx, sx > 0 ? chx_r : (sx < 0 ? chx_l : chx));
@@ -256,6 +263,11 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
         er_prev = er;
       }
     }
+    };
+    if ((p.reflect & 3u) == 0 && flatten)
+      walk(std::true_type{});
+    else
+      walk(std::false_type{});
   }
 }
 

@@ -116,12 +116,17 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     bool f = false;
     ct_pre = __ldg(xc + base + mirror_index(k_first - 3, nr, f) * rs + gx);
   }
-  // the walk, with the reflective flips compiled out when no end reflects
-  auto walk = [&](auto refl) {
-  constexpr bool RF = decltype(refl)::value;
+  // the walk; its common form (FAST: no reflective end in the walk's two
+  // dimensions, MUSCL with flattening) has the reflective flips and the
+  // reconstruction tests compiled out
+  auto walk = [&](auto fast) {
+  constexpr bool FAST = decltype(fast)::value;
+  constexpr bool RF = !FAST;
+  const bool flat = FAST || flatten;
+  const bool mus = FAST || muscl;
   for (int64_t k = k_first; k <= k_last; ++k) {
     const T ct = ct_pre;
-    if (flatten && k < k_last) {
+    if (flat && k < k_last) {
       bool f = false;
       ct_pre = __ldg(xc + base + mirror_index(k - 2, nr, f) * rs + gx);
     }
@@ -156,7 +161,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     CHY[1] = CHY[2];
     // re-derived: the same products derive() formed when the rows were loaded
     const T rinv1 = kRederive ? fl_rcp<T>(U[1].v[0]) : T(0);
-    if (flatten) {
+    if (flat) {
       if constexpr (kRederive)
         CHY[2] = (T)chi_base<T>(P[3], P[1], P[4], P[0], U[1].v[2 + DR] * rinv1,
                                 U[3].v[2 + DR] * fl_rcp<T>(U[3].v[0]));
@@ -172,17 +177,17 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     const T p_r1 = shfl_dn(pj, 1), p_l1 = shfl_up(pj, 1);
     const T p_r2 = shfl_dn(pj, 2), p_l2 = shfl_up(pj, 2);
     T chx = T(1);
-    if (flatten) chx = (T)chi_base<T>(p_r1, p_l1, p_r2, p_l2, shfl_up(vxj, 1), shfl_dn(vxj, 1));
+    if (flat) chx = (T)chi_base<T>(p_r1, p_l1, p_r2, p_l2, shfl_up(vxj, 1), shfl_dn(vxj, 1));
     const T chx_r = shfl_dn(chx, 1), chx_l = shfl_up(chx, 1);
 
     const Cons<T, D>& u = U[1];
     Cons<T, D> er, el;
-    if (!muscl) {
+    if (!mus) {
       er = u;
       el = u;
     } else {
       T chi_v = T(1);
-      if (flatten) {
+      if (flat) {
         const T dx = p_r1 - p_l1;
         const int sx = (T(0) < dx) - (dx < T(0));
         const T cx = std_min(chx, sx > 0 ? chx_r : (sx < 0 ? chx_l : chx));
@@ -269,7 +274,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     }
   }
   };
-  if ((p.reflect & (1u | (1u << DR))) != 0)
+  if ((p.reflect & (1u | (1u << DR))) == 0 && flatten)
     walk(std::true_type{});
   else
     walk(std::false_type{});
