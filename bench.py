@@ -40,10 +40,10 @@ GAMMA = 1.4
 SEED = 0
 # DRAM bytes (read + write) per cell of one sweep launch, measured by ncu at
 # 4096^2 on four consecutive launches of the headline loop (FP64 HLLC,
-# staged_walk_2d x and y sweeps of the alternating-layout loop: 602.2 MB read
-# + 494.5 MB written per launch on average, 1,096.7 MB against 1,073.7 MB
-# algorithmic; profiles/staged_walk_2d_f64_hllc_4096sq_launches.md).
-MEASURED_TRAFFIC_PER_CELL = {("f64", "hllc"): 1096.7e6 / 4096 ** 2}
+# staged_walk_2d x and y sweeps of the alternating-layout loop: 608.6 MB read
+# + 496.1 MB written per launch on average, 1,104.7 MB against 1,073.7 MB
+# algorithmic; profiles/staged_walk_2d_f64_hllc_4096sq.md).
+MEASURED_TRAFFIC_PER_CELL = {("f64", "hllc"): 1104.7e6 / 4096 ** 2}
 
 
 def parse():
