@@ -45,6 +45,7 @@
 #define FL_STAGED_RY 64
 #endif
 
+
 namespace fl {
 
 // GEO = 1: the walk runs along the slow dimension of the input's layout and a
@@ -91,7 +92,9 @@ struct StagedCfg {
   static constexpr size_t SMEM = WARPS * WARP_BYTES + 128;
   static_assert(STAGE_BYTES % 128 == 0 && (OUT * sizeof(T)) % 128 == 0, "128-byte boxes");
   // registers held to this many resident CTAs per SM
-  static constexpr int MIN_CTAS = (sizeof(T) == 8) ? (GEO ? 4 : 7) : (GEO ? 6 : 4);
+  // (FP32 rows: 5, as many as their shared memory allows; 6 held the
+  // registers to 80 for no resident CTA more, 1.3% slower)
+  static constexpr int MIN_CTAS = (sizeof(T) == 8) ? (GEO ? 4 : 7) : (GEO ? 5 : 4);
   static_assert(NS >= LIVE + 1, "the ring needs room to prefetch");
 };
 
@@ -272,8 +275,10 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   const int64_t pitch = p.pitch;
 
   // the walk, with the limiter kind fixed for the whole strip.  Its common
-  // form (FAST: no end of either dimension reflects, MUSCL with flattening)
-  // has the reflective flips and the reconstruction tests compiled out.
+  // form (FAST: no end of either dimension reflects, MUSCL with flattening,
+  // the wavespeed folded in the y sweep only and over every row) has the
+  // reflective flips and the reconstruction and wavespeed tests compiled
+  // out.
   auto walk = [&](auto lim, auto fast) {
   constexpr int LIM = decltype(lim)::value;
   constexpr bool FAST = decltype(fast)::value;
@@ -441,7 +446,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
             }
           }
         }
-        if (want_ws && owned && ws_row_counts(p, S == 1 ? jo : ai))
+        if ((FAST ? S == 1 : want_ws) && owned && (FAST || ws_row_counts(p, S == 1 ? jo : ai)))
           ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(res, gm1), gamma, pinf));
       }
       f_prev = fj;
@@ -451,7 +456,7 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
   };
   using SB = std::integral_constant<int, kSuperbee>;
   using VL_ = std::integral_constant<int, kVanLeer>;
-  if (!flip_l_on && !flip_a_on && flatten) {
+  if (!flip_l_on && !flip_a_on && flatten && want_ws == (S == 1) && p.ws_hi <= p.ws_lo) {
     if (p.limiter == kSuperbee)
       walk(SB{}, std::true_type{});
     else
