@@ -20,9 +20,11 @@
 // lane 0 keeps the ring filled ahead of the walk.  The stencil along the
 // sweep reads the ring (own lane only, no exchange).  The stencil across the
 // sweep -- the flattening coefficient's pressure and velocity reach of 3 --
-// goes through three small per-warp exchange rows; the 6 across-halo cells
-// (3 on each side of the warp) are derived in one extra pass of all lanes, of
-// which lanes 0-5 keep theirs (no divergent region).
+// goes through two small per-warp exchange rows (pressure and velocity);
+// the 6 across-halo cells (3 on each side of the warp) are derived in one
+// extra pass of all lanes, of which lanes 0-5 keep theirs (no divergent
+// region), and each lane computes the flattening base of the neighbour its
+// pressure rises towards itself, from those rows.
 // The reference's halo of 4 along the sweep costs 7 extra derivations per
 // strip of 64 and one extra evolve and Riemann solve at its start.
 //
@@ -83,7 +85,7 @@ struct StagedCfg {
   static constexpr int NOUT = TOUT ? (GEO ? 1 : 2) : 0;
   static constexpr size_t RING_BYTES = (size_t)NS * STAGE_BYTES;
   static constexpr size_t OUT_BYTES = (size_t)NOUT * OUT * sizeof(T);
-  static constexpr size_t X_BYTES = 3 * 40 * sizeof(T);
+  static constexpr size_t X_BYTES = 2 * 40 * sizeof(T);
   static constexpr size_t BAR_BYTES = NS * 8;
   static constexpr size_t WARP_BYTES =
       (RING_BYTES + OUT_BYTES + X_BYTES + BAR_BYTES + 127) / 128 * 128;
@@ -106,14 +108,12 @@ struct StagedSmem {
   T* out;
   T* xp;   // pressure across the warp, by box index
   T* xv;   // velocity across the sweep, by box index
-  T* xc;   // flattening base across the sweep, by box index
   uint64_t* bars;
   __device__ __forceinline__ explicit StagedSmem(unsigned char* base) {
     ring = reinterpret_cast<T*>(base);
     out = reinterpret_cast<T*>(base + C::RING_BYTES);
     xp = reinterpret_cast<T*>(base + C::RING_BYTES + C::OUT_BYTES);
     xv = xp + 40;
-    xc = xv + 40;
     bars = reinterpret_cast<uint64_t*>(base + C::RING_BYTES + C::OUT_BYTES + C::X_BYTES);
   }
 };
@@ -338,20 +338,20 @@ __device__ __forceinline__ void staged_strip(const SweepParams& p, const CUtenso
       }
       __syncwarp();
       const T pr1 = sm.xp[own + 1], pl1 = sm.xp[own - 1];
-      const T chx = (T)chi_base<T>(pr1, pl1, sm.xp[own + 2], sm.xp[own - 2], sm.xv[own - 1],
-                                   sm.xv[own + 1]);
-      sm.xc[own] = chx;
-      {
-        // lanes 0 and 1: the flattening base just outside the warp
-        const int o = (lane == 0) ? Cf::AOFF - 1 : Cf::AOFF + 32;
-        const T ce = (T)chi_base<T>(sm.xp[o + 1], sm.xp[o - 1], sm.xp[o + 2], sm.xp[o - 2],
-                                    sm.xv[o - 1], sm.xv[o + 1]);
-        if (lane < 2) sm.xc[o] = ce;
-      }
+      const T pr2 = sm.xp[own + 2], pl2 = sm.xp[own - 2];
+      const T vr1 = sm.xv[own + 1], vl1 = sm.xv[own - 1];
       const T dx = pr1 - pl1;
       const int sx = (T(0) < dx) - (dx < T(0));
-      __syncwarp();
-      cx = std_min(chx, sx > 0 ? sm.xc[own + 1] : (sx < 0 ? sm.xc[own - 1] : chx));
+      // the two values the neighbour the pressure rises towards needs beyond
+      // this lane's own reach
+      const T p3 = sm.xp[own + 3 * sx], v2 = sm.xv[own + 2 * sx];
+      __syncwarp();  // every lane has read the exchange rows
+      const T chx = (T)chi_base<T>(pr1, pl1, pr2, pl2, vl1, vr1);
+      const T qp = q.p, qv = q.v[1 - S];
+      const bool upw = sx > 0;
+      const T cn = (T)chi_base<T>(upw ? pr2 : qp, upw ? qp : pl2, upw ? p3 : pr1, upw ? pl1 : p3,
+                                  upw ? qv : v2, upw ? v2 : qv);
+      cx = std_min(chx, sx != 0 ? cn : chx);
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) CX[i] = CX[i + 1];
