@@ -122,8 +122,8 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
     }
     // the walk; its common form (FAST: no reflective end in x or y, MUSCL
-    // with flattening) has the reflective flips and the reconstruction tests
-    // compiled out
+    // with flattening and the van Leer limiter) has the reflective flips and
+    // the reconstruction and limiter tests compiled out
     auto walk = [&](auto fast) {
     constexpr bool FAST = decltype(fast)::value;
     const bool flat = FAST || flatten;
@@ -206,7 +206,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
             b.v[c] = u.v[c] + delta;
           }
         };
-        if (p.limiter == kSuperbee)
+        if (!FAST && p.limiter == kSuperbee)
           slopes(std::integral_constant<int, kSuperbee>{});
         else
           slopes(std::integral_constant<int, kVanLeer>{});
@@ -264,7 +264,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       }
     }
     };
-    if ((p.reflect & 3u) == 0 && flatten)
+    if ((p.reflect & 3u) == 0 && flatten && p.limiter == kVanLeer)
       walk(std::true_type{});
     else
       walk(std::false_type{});

@@ -117,8 +117,8 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     ct_pre = __ldg(xc + base + mirror_index(k_first - 3, nr, f) * rs + gx);
   }
   // the walk; its common form (FAST: no reflective end in the walk's two
-  // dimensions, MUSCL with flattening) has the reflective flips and the
-  // reconstruction tests compiled out
+  // dimensions, MUSCL with flattening and the van Leer limiter) has the
+  // reflective flips and the reconstruction and limiter tests compiled out
   auto walk = [&](auto fast) {
   constexpr bool FAST = decltype(fast)::value;
   constexpr bool RF = !FAST;
@@ -218,7 +218,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
           b.v[c] = u.v[c] + delta;
         }
       };
-      if (p.limiter == kSuperbee)
+      if (!FAST && p.limiter == kSuperbee)
         slopes(std::integral_constant<int, kSuperbee>{});
       else
         slopes(std::integral_constant<int, kVanLeer>{});
@@ -274,7 +274,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     }
   }
   };
-  if ((p.reflect & (1u | (1u << DR))) == 0 && flatten)
+  if ((p.reflect & (1u | (1u << DR))) == 0 && flatten && p.limiter == kVanLeer)
     walk(std::true_type{});
   else
     walk(std::false_type{});
