@@ -122,8 +122,11 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       for (int c = 0; c < NC; ++c) pre.v[c] = __ldg(in + c * pitch + gy * n0 + gx);
     }
     // the walk; its common form (FAST: no reflective end in x or y, MUSCL
-    // with flattening and the van Leer limiter) has the reflective flips and
-    // the reconstruction and limiter tests compiled out
+    // with flattening and the van Leer limiter, the wavespeed in the y sweep
+    // only) has the reflective flips and the reconstruction, limiter and
+    // wavespeed tests compiled out.  A slab's row window for the wavespeed
+    // stays a runtime test, so that slabs take the same code as the
+    // undivided grid and match it bit for bit.
     auto walk = [&](auto fast) {
     constexpr bool FAST = decltype(fast)::value;
     const bool flat = FAST || flatten;
@@ -238,7 +241,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
           const int64_t gi = j * n0 + x;
 #pragma unroll
           for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-          if (want_ws && ws_row_counts(p, j))
+          if ((FAST ? S == 1 : want_ws) && ws_row_counts(p, j))
             ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
         }
       } else {
@@ -255,7 +258,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
             const int64_t gi = (j - 1) * n0 + x;
 #pragma unroll
             for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-            if (want_ws && ws_row_counts(p, j - 1))
+            if ((FAST ? S == 1 : want_ws) && ws_row_counts(p, j - 1))
               ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
           }
           f_prev = fxy;
@@ -264,7 +267,7 @@ __device__ __forceinline__ void walk_strip_2d(const SweepParams& p, T dtdh, int6
       }
     }
     };
-    if ((p.reflect & 3u) == 0 && flatten && p.limiter == kVanLeer)
+    if ((p.reflect & 3u) == 0 && flatten && p.limiter == kVanLeer && want_ws == (S == 1))
       walk(std::true_type{});
     else
       walk(std::false_type{});
