@@ -117,8 +117,9 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     ct_pre = __ldg(xc + base + mirror_index(k_first - 3, nr, f) * rs + gx);
   }
   // the walk; its common form (FAST: no reflective end in the walk's two
-  // dimensions, MUSCL with flattening and the van Leer limiter) has the
-  // reflective flips and the reconstruction and limiter tests compiled out
+  // dimensions, MUSCL with flattening and the van Leer limiter, the
+  // wavespeed in the z sweep only) has the reflective flips and the
+  // reconstruction, limiter and wavespeed tests compiled out
   auto walk = [&](auto fast) {
   constexpr bool FAST = decltype(fast)::value;
   constexpr bool RF = !FAST;
@@ -249,7 +250,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
         const int64_t gi = base + j * rs + x;
 #pragma unroll
         for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-        if (want_ws)
+        if (FAST ? S == 2 : want_ws)
           ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
       }
     } else {
@@ -265,7 +266,7 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
           const int64_t gi = base + (j - 1) * rs + x;
 #pragma unroll
           for (int c = 0; c < NC; ++c) out[c * pitch + gi] = r.v[c];
-          if (want_ws)
+          if (FAST ? S == 2 : want_ws)
             ws_max(ws_local, (double)max_wavespeed_q<STIFF>(derive(r, gm1), gamma, pinf));
         }
         f_prev = fxy;
@@ -274,7 +275,8 @@ __device__ __forceinline__ void walk_strip_3d(const SweepParams& p, const T* __r
     }
   }
   };
-  if ((p.reflect & (1u | (1u << DR))) == 0 && flatten && p.limiter == kVanLeer)
+  if ((p.reflect & (1u | (1u << DR))) == 0 && flatten && p.limiter == kVanLeer &&
+      want_ws == (S == 2))
     walk(std::true_type{});
   else
     walk(std::false_type{});
